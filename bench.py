@@ -1,0 +1,387 @@
+"""Benchmark: RK steps/s of the quasi-dynamic SEAS step at ~60k triangles.
+
+Workload ("curved60k"): 150 km rough vertical strike-slip fault + 40 km branch
+at 20 degrees, 59,696 triangles, H-matrix leaf 64, eta 2, ACA relative tol 1e-5;
+operator stored BF16 (low rank) + FP32 (near field), FP64 state and slip;
+reference-mode DP5(4) stepping (one H-matvec per step, frozen load).
+
+A step = one H-matvec of the slip-rate deficit + one fused DP5(4) step kernel
+(accept/reject loop on the device).  The printed JSON line reports:
+  value       steps/s of the mixed-precision path, state resident in HBM
+  e2e         steps/s through QDsim.simu_forward (the reference call), with the
+              per-step host traffic of the reference main loop (dttry in; h,
+              dtnext and max slip rates out; slip-rate and traction vectors out)
+  plain_fp64  the same step with the FP64 operator (the plain GPU path)
+  roofline    H-matvec algorithmic bytes / measured duration vs measured HBM peak
+  cpu_baseline the reference's CPU step (six block-loop MVMs + DP5(4), oracle
+              port) on the same operator, bounded sample, on the host cores
+--impl reference runs only that CPU arm (all host cores, the reference's MPI
+block split emulated with worker processes) and prints its own line.
+Multi-GPU (torchrun): every rank simulates its own fault replica (independent
+ensemble members, no data-path collective); value = sum over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+
+CASE = "curved60k"
+METRIC = "RK steps/s and H-matvec HBM GB/s at 60k tris, mixed vs FP64 plain @1e-5 slip"
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_case(rank=0):
+    from pyquake3d_b200 import meshgen
+    d = os.path.join(tempfile.gettempdir(), "pq3d_bench_%s_r%d" % (CASE, rank))
+    msh = os.path.join(d, CASE + ".msh")
+    para = os.path.join(d, "parameter.txt")
+    if not (os.path.exists(msh) and os.path.exists(para)):
+        meshgen.make_case(CASE, d)
+    return msh, para
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + q, "--format=csv,noheader,nounits", "-lms", "200",
+                                       "-i", str(gpu_index)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        rows = [l.strip().split(", ") for l in open(self.f.name) if l.strip()]
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def export_host_operator(op):
+    import qd_oracle
+    from pyquake3d_b200.hmatrix import export_blocks
+    ho = object.__new__(qd_oracle.OracleOperator)
+    ho.blocks = export_blocks(op)
+    return ho
+
+
+def cpu_reference_steps(ho, state, V0, mu, Cs, budget_s, max_steps=20):
+    """The reference's step (oracle port) on the host: returns (steps/s, steps, seconds)."""
+    import qd_oracle
+    st = qd_oracle.OracleStepper(state, qd_oracle.operator_mvm(ho), V0, mu, Cs)
+    dttry = 1e-3
+    t0 = time.perf_counter()
+    k = 0
+    while k < max_steps:
+        _, dttry = st.simu_forward(dttry)
+        k += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return k / dt, k, dt
+
+
+# --------------------------------------------------------------------- reference arm (CPU)
+_W = {}
+
+
+def _worker_init(blocks):
+    _W["blocks"] = blocks
+
+
+def _worker_mvm(args):
+    import qd_oracle
+    x1, x2 = args
+    ho = object.__new__(qd_oracle.OracleOperator)
+    ho.blocks = _W["blocks"]
+    return qd_oracle.operator_mvm(ho)(x1, x2)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        print(json.dumps({"impl": "reference", "rank": rank, "skipped": "rank 0 runs the CPU arm"}), file=sys.stderr)
+        return
+    import multiprocessing as mp
+    import torch
+    import qd_oracle
+    from pyquake3d_b200 import QDsim, read_mshV2
+    msh, para = make_case(rank)
+    nodes, tris = read_mshV2(msh)
+    sim = QDsim(tris, nodes, para, device="cuda:0", precision="fp64")
+    # The operator values are produced on the device (CPU assembly at this size takes
+    # about an hour) and copied to the host; everything timed below runs on the CPU.
+    ho = export_host_operator(sim.tree_block.op())
+    del sim.tree_block._op
+    torch.cuda.empty_cache()
+    cores = os.cpu_count() or 1
+    nproc = max(1, min(cores, 32))
+    chunks = [ho.blocks[i::nproc] for i in range(nproc)]
+    ctx = mp.get_context("spawn")
+    pools = [ctx.Pool(1, initializer=_worker_init, initargs=(c,)) for c in chunks]
+
+    def mvm(x1, x2):
+        res = [p.apply_async(_worker_mvm, ((x1, x2),)) for p in pools]
+        parts = [r.get() for r in res]
+        return tuple(sum(p[k] for p in parts) for k in range(3))   # the reference's reduce(SUM)
+
+    st = qd_oracle.OracleStepper(qd_oracle.sim_state(sim), mvm, sim.V0, sim.mu, sim.Cs)
+    dttry = sim.htry
+    for _ in range(max(1, min(args.warmup, 2))):
+        _, dttry = st.simu_forward(dttry)
+    nsteps = max(1, min(args.steps, 10))
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        _, dttry = st.simu_forward(dttry)
+    dt = time.perf_counter() - t0
+    for p in pools:
+        p.close()
+    v = nsteps / dt
+    line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "steps/s", "n_gpus": world,
+            "steps": nsteps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / nsteps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": CASE + " (59,696 triangles, H-matrix leaf 64, eta 2, ACA rel 1e-5)",
+                       "path": "reference CPU step: six block-loop MVMs (MPI block split emulated by %d worker "
+                               "processes + sum) and DP5(4) in numpy, FP64" % nproc},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": nproc, "kind": "port",
+                             "sample": "%d steps of the 60k case after warm-up" % nsteps},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# --------------------------------------------------------------------- our arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    from pyquake3d_b200 import QDsim, read_mshV2
+    from pyquake3d_b200.qdsim import DeviceStepper
+    msh, para = make_case(rank)
+    nodes, tris = read_mshV2(msh)
+    t0 = time.perf_counter()
+    sim = QDsim(tris, nodes, para, device="cuda:%d" % local, precision="bf16")
+    t_host = time.perf_counter() - t0
+    op = sim.tree_block.op()
+    t_asm = time.perf_counter() - t0 - t_host
+    kS, kD = op.ranks()
+    mixed = DeviceStepper(sim, op, "bf16")
+    plain = DeviceStepper(sim, op, "fp64")
+    P_m, P_p = op.plan("bf16"), op.plan("fp64")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_steps(stepper, k, dttry):
+        stepper.set_history(k)
+        stepper.ctrl[0] = dttry
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(k):
+            stepper.launch(i)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        c = stepper.ctrl.cpu().numpy()
+        if c[4] != 0:
+            raise RuntimeError("step failed with status %d" % int(c[4]))
+        return e0.elapsed_time(e1) / 1e3, float(c[0])
+
+    # warm-up (both paths), then the timed mixed-precision region with clock sampling
+    dt_m = dt_p = sim.htry
+    _, dt_m = timed_steps(mixed, args.warmup, dt_m)
+    _, dt_p = timed_steps(plain, args.warmup, dt_p)
+    clk = Clocks(local)
+    t_mixed, dt_m = timed_steps(mixed, args.steps, dt_m)
+    clocks = clk.stop()
+    t_mixed = max_over_ranks(t_mixed)
+    hist_m = mixed.hist.view(-1, 6).cpu().numpy()[:args.steps]
+    t_plain, dt_p = timed_steps(plain, args.steps, dt_p)
+    t_plain = max_over_ranks(t_plain)
+    steps_total = args.steps * world
+    value = steps_total / t_mixed
+
+    # H-matvec alone (the dominant kernel sequence), CUDA events on the launching stream
+    def time_matvec(stepper, P, reps=50):
+        for _ in range(5):
+            op.matvec(stepper.x, stepper.precision, y=stepper.y)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            op.matvec(stepper.x, stepper.precision, y=stepper.y)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+    t_mv_m = time_matvec(mixed, P_m)
+    t_mv_p = time_matvec(plain, P_p)
+    hbm, peak_kind = peaks()
+    gbs_m = P_m["alg_bytes"] / t_mv_m / 1e9
+    gbs_p = P_p["alg_bytes"] / t_mv_p / 1e9
+
+    # slip error of the mixed path vs the FP64 path at equal times (dt replay)
+    rep_p = DeviceStepper(sim, op, "fp64")
+    rep_m = DeviceStepper(sim, op, "bf16")
+    nrep = min(args.steps, 500)
+    rep_p.set_history(nrep)
+    rep_p.ctrl[0] = sim.htry
+    for i in range(nrep):
+        rep_p.launch(i)
+    rep_m.set_replay(rep_p.hist.view(-1, 6)[:, 0])
+    rep_m.ctrl[0] = sim.htry
+    for i in range(nrep):
+        rep_m.launch(i)
+    torch.cuda.synchronize()
+    s_p = torch.sqrt(rep_p.t["slip1"] ** 2 + rep_p.t["slip2"] ** 2)
+    s_m = torch.sqrt(rep_m.t["slip1"] ** 2 + rep_m.t["slip2"] ** 2)
+    slip_err = float(torch.linalg.norm(s_m - s_p) / torch.linalg.norm(s_p))
+    v_err = float(torch.linalg.norm(rep_m.t["slipv"] - rep_p.t["slipv"]) / torch.linalg.norm(rep_p.t["slipv"]))
+    th_p = rep_p.t["psi"]
+    th_err = float(torch.linalg.norm(rep_m.t["psi"] - th_p) / torch.linalg.norm(th_p))
+    del rep_p, rep_m
+
+    # end to end through the reference call surface (QDsim.simu_forward) with the
+    # reference main loop's per-step host traffic
+    sim._dev = mixed
+    ne = min(args.steps, 300)
+    perm_t = torch.as_tensor(op.s.iperm, device=op.dev)
+    pin_v = torch.empty(sim.xg.shape[0], dtype=torch.float64).pin_memory()
+    pin_t = torch.empty_like(pin_v).pin_memory()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    dttry = dt_m
+    for _ in range(ne):
+        h, dttry = sim.simu_forward(dttry)
+        pin_v.copy_(mixed.t["slipv"].index_select(0, perm_t), non_blocking=True)
+        pin_t.copy_(mixed.t["Tt"].index_select(0, perm_t), non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    e2e = {"value": ne * world / t_e2e, "unit": "steps/s", "h2d_bytes_per_step": 8,
+           "d2h_bytes_per_step": int(16 * 8 + 2 * 8 * sim.xg.shape[0]),
+           "path": "QDsim.simu_forward per step + slip-rate and traction vectors to pinned host memory"}
+
+    # CPU baseline: the reference's step on the same operator (rank 0, N=1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        import qd_oracle
+        from pyquake3d_b200 import QDsim as Q2
+        ho = export_host_operator(op)
+        host = Q2(tris, nodes, para, device="cuda:0", precision="bf16")
+        rate, k, secs = cpu_reference_steps(ho, qd_oracle.sim_state(host), host.V0, host.mu, host.Cs,
+                                            args.cpu_budget)
+        cpu = {"value": rate, "unit": "steps/s", "cores": 1, "kind": "port",
+               "sample": "%d steps (%.1f s) of the same 60k workload: six block-loop MVMs + DP5(4), "
+                         "numpy FP64, one process" % (k, secs)}
+        del ho
+
+    traffic = None
+    tp = os.path.join(REPO, "profiles", "hmatvec_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("bytes_per_matvec_bf16")
+        except (ValueError, OSError):
+            traffic = None
+    nlaunch_step = (4 if P_m["n_lr"] > 0 else 2) + 1
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32 operator, f64 state", "data": "synthetic",
+        "config": {"workload": CASE + " (%d triangles: 150 km rough strike-slip fault + 40 km branch at 20 deg)"
+                               % sim.xg.shape[0],
+                   "precision": "bf16 low-rank / fp32 near-field / fp64 state", "leaf": 64, "eta": 2.0,
+                   "aca": "relative 1e-5", "mean_rank": float(np.mean(np.concatenate([kS, kD]))),
+                   "max_rank": int(max(kS.max(), kD.max())),
+                   "operator_bytes_bf16": int(P_m["stored_bytes"]), "operator_bytes_fp64": int(P_p["stored_bytes"]),
+                   "l2": "inputs larger than L2 (operator %.2f GB per step)" % (P_m["alg_bytes"] / 1e9),
+                   "parallelism": "replicas x%d" % world, "host_setup_s": round(t_host, 2),
+                   "assembly_s": round(t_asm, 2), "assembly_breakdown": {k: round(v, 3) for k, v in op.timings.items()}},
+        "roofline": {"bound": "hbm", "achieved": gbs_m, "peak": hbm, "unit": "GB/s", "frac": gbs_m / hbm,
+                     "traffic": traffic, "kernel": "H-matvec (4 launches), bf16/fp32",
+                     "alg_bytes": int(P_m["alg_bytes"]), "ms": 1e3 * t_mv_m, "peak_source": peak_kind},
+        "plain_fp64": {"steps_per_s": steps_total / t_plain, "ms_per_step": 1e3 * t_plain / args.steps,
+                       "hmatvec_GBs": gbs_p, "hmatvec_ms": 1e3 * t_mv_p, "alg_bytes": int(P_p["alg_bytes"]),
+                       "frac": gbs_p / hbm},
+        "mixed_vs_plain": (steps_total / t_mixed) / (steps_total / t_plain),
+        "accuracy_vs_fp64": {"slip_rel_l2": slip_err, "V_rel_l2": v_err, "psi_rel_l2": th_err,
+                             "steps": nrep, "method": "dt replay of the FP64 run"},
+        "sim": {"time_s": float(hist_m[-1, 2]), "last_dt": float(hist_m[-1, 0]),
+                "rejects": int(hist_m[:, 5].sum())},
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "gpu_launches": nlaunch_step * args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,144 @@
+/*
+ * pq3d: B200 (sm_100a) kernels for PyQuake3D's quasi-dynamic SEAS hot path.
+ *
+ * C ABI of libpq3d.so (pyquake3d_b200/libpq3d.so).  Plain pointers and sizes only.
+ * Two groups of entry points:
+ *
+ *  1. Host-pointer drop-ins with the exact signatures the reference binds with
+ *     ctypes (src/Hmatrix.py:22-49).  They stage the inputs to the GPU, run the
+ *     FP64 Green's-function kernel and copy the result back before returning.
+ *
+ *  2. Device entry points (prefix pq3d_): device pointers + a cudaStream_t,
+ *     return 0 (PQ3D_OK) or a negative error code, never exit or trap.  They
+ *     are stream-ordered and do not synchronize the host.
+ *
+ * All element vectors handed to the H-matrix and stepper entry points are in
+ * cluster-tree order (depth-first, left-first walk of the geometric cluster
+ * tree of src/Hmatrix.py:143-182), so every H-matrix block covers contiguous
+ * index ranges.
+ */
+#ifndef PQ3D_H
+#define PQ3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <stdbool.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PQ3D_OK 0
+#define PQ3D_ERR_ARG -1
+#define PQ3D_ERR_CUDA -2
+#define PQ3D_ERR_RANK -3
+#define PQ3D_ERR_DT -4
+#define PQ3D_ERR_TIMEOUT -5
+#define PQ3D_ERR_NOMEM -6
+
+/* ---------------------------------------------------------------- drop-ins */
+
+/* Replaces TDstressFS_C (src/TDstressFS_C.cpp:2048-2095): stress and strain
+ * (xx,yy,zz,xy,xz,yz per receiver, stress[i*6+c]) at n receivers (X,Y,Z) from one
+ * triangular dislocation P1,P2,P3 with Burgers components (Ss strike, Ds dip,
+ * Ts tensile).  Full space only: jud_halfspace=true is rejected (outputs NaN,
+ * message on stderr). */
+void TDstressFS_C(const double *X, const double *Y, const double *Z, size_t n,
+                  const double *P1, const double *P2, const double *P3,
+                  double Ss, double Ds, double Ts, double mu, double lambda_,
+                  bool jud_halfspace, double *stress, double *strain);
+
+/* Replaces TDstressEachSourceAtReceiver_C (src/TDstressFS_C.cpp:2098-2143): one
+ * receiver (x,y,z), n_sources triangles given as flat xyz triplets. */
+void TDstressEachSourceAtReceiver_C(double x, double y, double z,
+                                    const double *P1_flat, const double *P2_flat,
+                                    const double *P3_flat, size_t n_sources,
+                                    double Ss, double Ds, double Ts, double mu,
+                                    double lambda_, bool jud_halfspace,
+                                    double *stress_out, double *strain_out);
+
+/* ---------------------------------------------------------------- Green's function */
+
+/* Bytes of one per-element source record. */
+size_t pq3d_src_record_bytes(void);
+
+/* Per-element source records (TD frame, local vertices, angles) for n_elem
+ * triangles; d_tri holds 1-based node ids (n_elem x 3), d_nodes xyz in metres.
+ * Replaces the per-call setup inside TDstressFS (src/TDstressFS_C.cpp:294-385). */
+int pq3d_src_records(const double *d_nodes, const int64_t *d_tri, int64_t n_elem,
+                     void *d_rec, cudaStream_t stream);
+
+/* Tractions (A1s,A2s,Bs,A1d,A2d,Bd) for npairs (receiver, source) element pairs:
+ * the entries BlockTree.calc_stressfunc_fromCS/CD compute (src/Hmatrix.py:425-511). */
+int pq3d_traction_pairs(const double *d_xg, const double *d_ev, const void *d_rec,
+                        const int64_t *d_rows, const int64_t *d_cols, int64_t npairs,
+                        double mu, double lam, double *d_out, cudaStream_t stream);
+
+/* Device form of both drop-ins: n_pts receivers x n_src sources, one of which is 1
+ * (or both equal: pairwise).  d_P is n_src x 9 (P1,P2,P3). */
+int pq3d_stress_points(const double *d_X, const double *d_Y, const double *d_Z, int64_t n_pts,
+                       const double *d_P, int64_t n_src, double Ss, double Ds, double Ts,
+                       double mu, double lam, int halfspace, double *d_stress,
+                       double *d_strain, cudaStream_t stream);
+
+/* ---------------------------------------------------------------- H-matrix assembly */
+
+/* Dense near-field blocks (the Mf_* matrices of BlockTree.ACA_worker,
+ * src/Hmatrix.py:1050-1063) written straight into the packed matvec layout.
+ * d_blocks: array of DenseBlock {int64 off64, off32; int32 m, n, r0, c0}. */
+int pq3d_dense_assemble(const double *d_xg, const double *d_ev, const void *d_rec,
+                        const int32_t *d_perm, const void *d_blocks, int64_t n_blocks,
+                        double mu, double lam, double *d_out64, float *d_out32,
+                        cudaStream_t stream);
+
+/* Workspace (doubles) of one ACA task with rank cap kmax. */
+int64_t pq3d_aca_ws_doubles(int m, int n, int kmax);
+size_t pq3d_aca_task_bytes(void);
+size_t pq3d_pack_task_bytes(void);
+
+/* Batched ACA+ (BlockTree.ACA_plus_full_traceS/D, src/Hmatrix.py:581-1011), one
+ * CTA per (block, slip pass).  eps: absolute step-size tolerance (rel_mode 0, the
+ * reference's 0.01) or relative Frobenius tolerance (rel_mode 1).  Writes the
+ * rank and a flag word (1 rank cap reached, 2 B factor all zero) per task. */
+int pq3d_aca_batched(const double *d_xg, const double *d_ev, const void *d_rec,
+                     const int32_t *d_rowlist, const int32_t *d_collist,
+                     const void *d_tasks, int64_t n_tasks, double *d_ws, double mu,
+                     double lam, double eps, int rel_mode, int max_mn, int32_t *d_rank,
+                     int32_t *d_flags, cudaStream_t stream);
+
+/* Pack ACA factors into the matvec layout; dtype 0 FP64, 1 FP32, 2 BF16. */
+int pq3d_aca_pack(const void *d_tasks, int64_t n_tasks, const double *d_ws,
+                  const int32_t *d_rowlist, const int32_t *d_collist, const int32_t *d_iperm,
+                  int dtype, void *d_U, void *d_V, cudaStream_t stream);
+
+/* ---------------------------------------------------------------- H-matvec */
+
+/* Sizes of the work-item records: kind 0 DenseItem, 1 VItem, 2 UItem, 3 TBlock,
+ * 4 DenseBlock, 5 the plan struct. */
+size_t pq3d_item_bytes(int kind);
+
+/* y (n x 3, FP64) = [A1s A1d; A2s A2d; Bs Bd] x (+ add0/add1/add2 per component).
+ * Replaces the six BlockTree.blocks_process_MVM calls of QDsim.simu_forward
+ * (src/Hmatrix.py:1445-1538, src/QDsim.py:906-917).  plan_host is a host copy of
+ * the plan (device pointers inside); x interleaved strike/dip deficit. */
+int pq3d_hmatvec(const void *plan_host, const void *d_x, void *d_slots, void *d_tpart,
+                 void *d_t, const double *d_add0, const double *d_add1,
+                 const double *d_add2, double *d_y, cudaStream_t stream);
+
+/* ---------------------------------------------------------------- stepper */
+
+size_t pq3d_rk_args_bytes(void);
+/* Co-resident grid size for the step kernel, for n elements. */
+int pq3d_rk_grid(int n);
+/* One DP5(4) step with frozen load (QDsim.simu_forward after the matvec and
+ * RungeKutte_solve_Dormand_Prince, src/QDsim.py:892-1134), cooperative launch.
+ * Control block ctrl: [0] dttry in / dtnext out, [1] accepted h, [2] time,
+ * [3] rejects this step, [4] status, [5] max|V1|, [6] max|V2|, [8] steps,
+ * [9] total rejects, [10] total attempts. */
+int pq3d_rk_step(const void *args, int grid, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PQ3D_H */

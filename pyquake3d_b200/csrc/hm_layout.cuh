@@ -1,0 +1,61 @@
+// Packed H-matrix layout shared by assembly, ACA packing and the matvec.
+//
+// All row/column indices are positions in cluster-tree order (a depth-first,
+// left-first walk of the cluster tree), so every block covers contiguous
+// ranges [r0, r0+m) x [c0, c0+n) and the operator needs no gather/scatter.
+//
+// Dense block (m x n, six operators): element (row i, col j, comp c, slip s)
+//   at  ((j / CW) * m + i) * 6*CW + (2*c + s) * CW + (j % CW)
+// with comp c in {tau1, tau2, sigma_n} and slip s in {strike, dip}; CW is 4
+// for FP32 and 2 for FP64, so one row's CW columns for all six operators are
+// 96 contiguous bytes and 32 consecutive rows are 3 KB contiguous.
+//
+// Low-rank block (ACA): for comp c the block is U_c T_c with
+//   U_c = [U_cs | U_cd]  (m x K, K = kS + kD, padded to a multiple of CWU)
+//   t_c = [V_cs x_strike ; V_cd x_dip]
+// U element (row i, comp c, q) at ((q / CWU) * m + i) * 3*CWU + c*CWU + q % CWU.
+// V rows: Q = 3*kS + 3*kD rows (A1s, A2s, Bs rows first, then A1d, A2d, Bd),
+// element (row q, col j) at ((j / CWV) * Q + q) * CWV + j % CWV.
+#pragma once
+#include <stdint.h>
+
+namespace pq3d {
+
+constexpr int kCW32 = 4;   // dense FP32 column group
+constexpr int kCW64 = 2;   // dense FP64 column group
+
+struct DenseBlock {
+    int64_t off64, off32;  // element offsets of the block in the FP64 / FP32 dense arrays
+    int32_t m, n, r0, c0;
+};
+
+__host__ __device__ inline int64_t dense_index(int m, int i, int j, int comp, int slip, int cw)
+{
+    return ((int64_t)(j / cw) * m + i) * (6 * cw) + (2 * comp + slip) * cw + (j % cw);
+}
+
+__host__ __device__ inline int64_t u_index(int m, int i, int comp, int q, int cwu)
+{
+    return ((int64_t)(q / cwu) * m + i) * (3 * cwu) + comp * cwu + (q % cwu);
+}
+
+__host__ __device__ inline int64_t v_index(int Q, int q, int j, int cwv)
+{
+    return ((int64_t)(j / cwv) * Q + q) * cwv + (j % cwv);
+}
+
+// Matvec work items (one warp each).
+struct DenseItem {          // rows [r, r+32) of a dense block, column groups [g0, g1)
+    int64_t off;            // block offset in the dense array
+    int32_t m, r, g0, g1, c0, slot;  // slot: slot index of block row 0 for this column chunk
+};
+struct VItem {              // V rows [q, q+32) of a low-rank block, column groups [g0, g1)
+    int64_t off;            // block offset in the V array
+    int32_t Q, q, g0, g1, c0, kS, tp;  // tp: offset of this chunk's partial t (Q values)
+};
+struct UItem {              // rows [r, r+32) of a low-rank block
+    int64_t off;            // block offset in the U array
+    int32_t m, r, K, kS, kD, slot, tp, nch;  // tp/nch: first chunk partial and chunk count (stride Q)
+};
+
+}  // namespace pq3d

@@ -1,0 +1,593 @@
+"""H-matrix structure (host) and the packed device operator.
+
+Host part (FP64, numpy), a restatement of src/Hmatrix.py:
+  * build_cluster_tree  <- build_block_tree   (:143-182)  bisection of the
+    longest bounding-box axis at its midpoint, leaves of <= min_size elements;
+  * is_admissible       <- is_admissible      (:88-103)   min(diam) <= eta*dist;
+  * build_blocks        <- create_recursive_blocks + collect_blocks (:1611-1672,
+    :1291-1297) quad-split, a leaf when admissible or when either cluster has
+    <= mini_leaf elements; leaves listed depth-first (the reference's order);
+  * ACA vs dense        <- BlockTree.ACA_worker (:1014-1066): ACA when both
+    dimensions exceed mini_leaf, dense otherwise.
+Every cluster is also given its range in tree order (depth-first, left child
+first), the layout of all device vectors.
+
+Device part: DeviceHMatrix assembles the operator on the GPU (dense near field
+with the FP64 Green's function, admissible blocks with batched ACA), packs it
+for one or more storage precisions and applies it with pq3d_hmatvec.
+"""
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import ptr, check
+
+# ----------------------------------------------------------------------------- host tree
+
+
+class ClusterNode:
+    __slots__ = ("indices", "left", "right", "start", "level", "bbox_min", "bbox_max", "leaf_id")
+
+    def __init__(self, indices, level):
+        self.indices = indices
+        self.left = None
+        self.right = None
+        self.start = 0
+        self.level = level
+        self.bbox_min = None
+        self.bbox_max = None
+        self.leaf_id = -1
+
+
+def build_cluster_tree(points, min_size=16):
+    """Cluster tree of build_block_tree (src/Hmatrix.py:143-182).
+
+    Returns (root, perm, leaves): perm[p] = element at tree position p."""
+    root = ClusterNode(np.arange(len(points)), 0)
+    stack = [(root, points)]
+    while stack:
+        node, pts = stack.pop()
+        cl = node.indices
+        node.bbox_min = np.min(pts, axis=0)
+        node.bbox_max = np.max(pts, axis=0)
+        if len(cl) <= min_size:
+            continue
+        alpha, beta = node.bbox_min, node.bbox_max
+        j = int(np.argmax(beta - alpha))
+        gamma = (alpha[j] + beta[j]) / 2
+        i1 = pts[:, j] <= gamma
+        i2 = pts[:, j] > gamma
+        t1, t2 = cl[i1], cl[i2]
+        if len(t1) == 0 or len(t2) == 0:
+            continue
+        node.left = ClusterNode(t1, node.level + 1)
+        node.right = ClusterNode(t2, node.level + 1)
+        stack.append((node.right, pts[i2]))
+        stack.append((node.left, pts[i1]))
+    # tree-order ranges (left first) and leaves
+    perm = np.empty(len(points), dtype=np.int64)
+    leaves = []
+    pos = 0
+    st = [root]
+    while st:
+        nd = st.pop()
+        nd.start = pos if nd.left is None else nd.start
+        if nd.left is None:
+            nd.start = pos
+            nd.leaf_id = len(leaves)
+            leaves.append(nd)
+            perm[pos:pos + len(nd.indices)] = nd.indices
+            pos += len(nd.indices)
+        else:
+            st.append(nd.right)
+            st.append(nd.left)
+    _fix_starts(root)
+    return root, perm, leaves
+
+
+def _fix_starts(root):
+    st = [root]
+    order = []
+    while st:
+        nd = st.pop()
+        order.append(nd)
+        if nd.left is not None:
+            st.append(nd.right)
+            st.append(nd.left)
+    for nd in reversed(order):
+        if nd.left is not None:
+            nd.start = nd.left.start
+
+
+def is_admissible(a, b, eta):
+    """min(diam_a, diam_b) <= eta * dist(bbox_a, bbox_b)."""
+    da = np.sqrt(np.sum((a.bbox_max - a.bbox_min) ** 2))
+    db = np.sqrt(np.sum((b.bbox_max - b.bbox_min) ** 2))
+    dq = np.sqrt(np.sum((np.maximum(0, b.bbox_min - a.bbox_max) ** 2) + (np.maximum(0, a.bbox_min - b.bbox_max) ** 2)))
+    return min(da, db) <= eta * dq
+
+
+class LeafBlock:
+    """A leaf of the block tree: rows = row cluster, cols = col cluster."""
+    __slots__ = ("row", "col", "aca", "admissible", "level")
+
+    def __init__(self, row, col, aca, admissible, level):
+        self.row = row
+        self.col = col
+        self.aca = aca
+        self.admissible = admissible
+        self.level = level
+
+    @property
+    def row_cluster(self):
+        return self.row.indices
+
+    @property
+    def col_cluster(self):
+        return self.col.indices
+
+    @property
+    def judaca(self):
+        return self.aca
+
+
+def build_blocks(row_root, col_root, eta=2.0, mini_leaf=32):
+    """Leaves of create_recursive_blocks in collect_blocks (depth-first) order."""
+    out = []
+    st = [(row_root, col_root, 0)]
+    while st:
+        r, c, lev = st.pop()
+        adm = is_admissible(r, c, eta)
+        if adm or len(r.indices) <= mini_leaf or len(c.indices) <= mini_leaf or \
+                r.left is None or r.right is None or c.left is None or c.right is None:
+            aca = len(r.indices) > mini_leaf and len(c.indices) > mini_leaf
+            out.append(LeafBlock(r, c, aca, bool(adm), lev))
+            continue
+        st.append((r.right, c.right, lev + 1))
+        st.append((r.right, c.left, lev + 1))
+        st.append((r.left, c.right, lev + 1))
+        st.append((r.left, c.left, lev + 1))
+    return out
+
+
+class HStructure:
+    """Cluster trees and leaf blocks of the operator (the part QDsim.__init__ builds)."""
+
+    def __init__(self, xg, mini_leaf=32, eta=2.0, min_size=16):
+        self.n = len(xg)
+        self.mini_leaf = mini_leaf
+        self.eta = eta
+        self.row_root, self.perm, self.leaves = build_cluster_tree(xg, min_size)
+        # the reference builds the column tree with the same call: identical tree
+        self.col_root = self.row_root
+        self.iperm = np.empty_like(self.perm)
+        self.iperm[self.perm] = np.arange(self.n)
+        self.blocks = build_blocks(self.row_root, self.col_root, eta, mini_leaf)
+
+    def stats(self):
+        nd = sum(1 for b in self.blocks if not b.aca)
+        na = len(self.blocks) - nd
+        dense_entries = sum(len(b.row.indices) * len(b.col.indices) for b in self.blocks if not b.aca)
+        aca_mn = sum(len(b.row.indices) + len(b.col.indices) for b in self.blocks if b.aca)
+        return dict(n=self.n, blocks=len(self.blocks), dense_blocks=nd, aca_blocks=na,
+                    dense_entries=dense_entries, aca_m_plus_n=aca_mn, leaves=len(self.leaves))
+
+
+def aca_start_indices(blocks, seed):
+    """Starting reference row/col of every ACA pass, drawn as the reference does
+    (np.random.randint(n_rows) - 3, np.random.randint(n_cols) - 3 for the strike
+    pass, then again for the dip pass, src/Hmatrix.py:660-661 and :888-889), with
+    a seeded legacy RandomState and blocks taken in list order."""
+    rs = np.random.RandomState(seed)
+    out = []
+    for b in blocks:
+        if not b.aca:
+            continue
+        m, n = len(b.row.indices), len(b.col.indices)
+        s = (rs.randint(m) - 3, rs.randint(n) - 3)
+        d = (rs.randint(m) - 3, rs.randint(n) - 3)
+        out.append((s, d))
+    return out
+
+
+# ----------------------------------------------------------------------------- device operator
+
+DTYPES = {"fp64": 0, "fp32": 1, "bf16": 2}
+_CW_DENSE = {0: 2, 1: 4, 2: 4}
+_CW_LR = {0: 2, 1: 4, 2: 8}
+
+
+def _cdiv(a, b):
+    return (a + b - 1) // b
+
+
+class DeviceHMatrix:
+    """The packed operator on one GPU.
+
+    assemble() computes dense blocks and ACA factors in FP64 on the device;
+    plan(dtype) packs them into the matvec layout of one storage precision
+    ("fp64": FP64 everywhere; "fp32": FP32 everywhere; "bf16": FP32 dense,
+    BF16 low rank).  matvec(x_dev, dtype) returns y (n x 3, FP64, tree order)."""
+
+    DENSE_CHUNK_GROUPS = 64   # column groups per dense work item
+    V_CHUNK_GROUPS = 64       # column groups per V work item
+
+    def __init__(self, struct, xg, ev, nodes, tri, mu, lam, device="cuda", aca_tol=0.01, aca_rel=False,
+                 aca_seed=0, kcap=96, ws_budget_bytes=8 << 30):
+        import torch
+        self.torch = torch
+        self.L = _lib.load()
+        self.s = struct
+        self.n = struct.n
+        self.mu, self.lam = float(mu), float(lam)
+        self.dev = torch.device(device)
+        self.aca_tol, self.aca_rel, self.aca_seed = float(aca_tol), bool(aca_rel), int(aca_seed)
+        self.kcap = int(kcap)
+        self.ws_budget = int(ws_budget_bytes)
+        f64 = dict(dtype=torch.float64, device=self.dev)
+        self.xg = torch.tensor(np.ascontiguousarray(xg), **f64)
+        self.ev = torch.tensor(np.ascontiguousarray(ev), **f64)
+        self.nodes = torch.tensor(np.ascontiguousarray(nodes), **f64)
+        self.tri = torch.tensor(np.ascontiguousarray(tri, dtype=np.int64), dtype=torch.int64, device=self.dev)
+        self.perm = torch.tensor(struct.perm.astype(np.int32), dtype=torch.int32, device=self.dev)
+        self.iperm = torch.tensor(struct.iperm.astype(np.int32), dtype=torch.int32, device=self.dev)
+        rb = self.L.pq3d_src_record_bytes()
+        self.rec = torch.empty((self.n * rb + 7) // 8, **f64)
+        self._stream = _lib.stream_ptr()
+        check(self.L.pq3d_src_records(ptr(self.nodes), ptr(self.tri), self.n, ptr(self.rec), self._stream),
+              "pq3d_src_records")
+        self.dense_blocks = [b for b in struct.blocks if not b.aca]
+        self.aca_blocks = [b for b in struct.blocks if b.aca]
+        self.plans = {}
+        self.assembled = False
+        self.timings = {}
+
+    # ------------------------------------------------------------------ assembly
+    def assemble(self, want=("fp64", "bf16")):
+        """Dense near field + ACA factors (FP64 on device), then pack for each dtype."""
+        import time
+        torch = self.torch
+        want = tuple(want)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        self._assemble_dense(want)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        self._run_aca()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        self.timings.update(dense_s=t1 - t0, aca_s=t2 - t1)
+        for d in want:
+            self.plan(d)
+        torch.cuda.synchronize()
+        self.timings["pack_s"] = time.perf_counter() - t2
+        self.assembled = True
+        return self
+
+    def _assemble_dense(self, want):
+        torch = self.torch
+        need64 = "fp64" in want
+        need32 = any(d in want for d in ("fp32", "bf16"))
+        recs = np.zeros(len(self.dense_blocks), dtype=_lib.DENSE_BLOCK)
+        off64 = off32 = 0
+        for i, b in enumerate(self.dense_blocks):
+            m, n = len(b.row.indices), len(b.col.indices)
+            recs[i] = (off64, off32, m, n, b.row.start, b.col.start)
+            off64 += _cdiv(n, 2) * m * 12
+            off32 += _cdiv(n, 4) * m * 24
+        order = np.argsort(-(recs["m"].astype(np.int64) * recs["n"]), kind="stable")
+        self.dense_recs = recs
+        self.dense64 = torch.zeros(max(off64, 1), dtype=torch.float64, device=self.dev) if need64 else None
+        self.dense32 = torch.zeros(max(off32, 1), dtype=torch.float32, device=self.dev) if need32 else None
+        if len(recs):
+            d_recs = torch.from_numpy(recs[order].view(np.uint8)).to(self.dev)
+            check(self.L.pq3d_dense_assemble(ptr(self.xg), ptr(self.ev), ptr(self.rec), ptr(self.perm), ptr(d_recs),
+                                             len(recs), self.mu, self.lam, ptr(self.dense64), ptr(self.dense32),
+                                             self._stream), "pq3d_dense_assemble")
+            torch.cuda.synchronize()
+
+    def _run_aca(self):
+        """Batched ACA over all admissible blocks; ranks and FP64 factors kept per task."""
+        torch = self.torch
+        starts = aca_start_indices(self.s.blocks, self.aca_seed)
+        rowlist, collist = [], []
+        tasks = []
+        roff = 0
+        for bi, b in enumerate(self.aca_blocks):
+            m, n = len(b.row.indices), len(b.col.indices)
+            rowlist.append(b.row.indices)
+            collist.append(b.col.indices)
+            for p in (0, 1):
+                tasks.append(dict(block=bi, pass_=p, m=m, n=n, rows_off=roff, cols_off=roff,
+                                  iref0=starts[bi][p][0], jref0=starts[bi][p][1]))
+            roff += 0  # offsets assigned below
+        # row and col lists stored separately
+        rl = np.concatenate(rowlist).astype(np.int32) if rowlist else np.zeros(1, np.int32)
+        cl = np.concatenate(collist).astype(np.int32) if collist else np.zeros(1, np.int32)
+        ro = np.concatenate([[0], np.cumsum([len(r) for r in rowlist])]).astype(np.int64) if rowlist else np.zeros(1, np.int64)
+        co = np.concatenate([[0], np.cumsum([len(c) for c in collist])]).astype(np.int64) if collist else np.zeros(1, np.int64)
+        for t in tasks:
+            t["rows_off"] = int(ro[t["block"]])
+            t["cols_off"] = int(co[t["block"]])
+        self.rowlist = torch.tensor(rl, dtype=torch.int32, device=self.dev)
+        self.collist = torch.tensor(cl, dtype=torch.int32, device=self.dev)
+        self.aca_tasks = tasks
+        self.aca_ranks = np.zeros(len(tasks), dtype=np.int32)
+        self.aca_flags = np.zeros(len(tasks), dtype=np.int32)
+        self.aca_ws = []  # (tensor, {task index: ws_off, kmax})
+        pending = list(range(len(tasks)))
+        kcap = self.kcap
+        while pending:
+            # batches bounded by the workspace budget, largest tasks first
+            pending.sort(key=lambda i: -(tasks[i]["m"] + tasks[i]["n"]))
+            retry = []
+            i0 = 0
+            while i0 < len(pending):
+                batch, ws_off = [], 0
+                while i0 < len(pending):
+                    t = tasks[pending[i0]]
+                    kmax = min(t["m"], t["n"], t.get("kcap", kcap))
+                    need = self.L.pq3d_aca_ws_doubles(t["m"], t["n"], kmax)
+                    if batch and (ws_off + need) * 8 > self.ws_budget:
+                        break
+                    batch.append((pending[i0], ws_off, kmax))
+                    ws_off += need
+                    i0 += 1
+                rec = np.zeros(len(batch), dtype=_lib.ACA_TASK)
+                max_mn = 0
+                for j, (ti, wo, kmax) in enumerate(batch):
+                    t = tasks[ti]
+                    rec[j] = (t["rows_off"], t["cols_off"], wo, t["m"], t["n"], kmax, t["pass_"], t["iref0"], t["jref0"])
+                    max_mn = max(max_mn, t["m"], t["n"])
+                ws = torch.empty(max(ws_off, 1), dtype=torch.float64, device=self.dev)
+                d_rec = torch.from_numpy(rec.view(np.uint8)).to(self.dev)
+                d_rank = torch.zeros(len(batch), dtype=torch.int32, device=self.dev)
+                d_flag = torch.zeros(len(batch), dtype=torch.int32, device=self.dev)
+                check(self.L.pq3d_aca_batched(ptr(self.xg), ptr(self.ev), ptr(self.rec), ptr(self.rowlist),
+                                              ptr(self.collist), ptr(d_rec), len(batch), ptr(ws), self.mu, self.lam,
+                                              self.aca_tol, 1 if self.aca_rel else 0, max_mn, ptr(d_rank),
+                                              ptr(d_flag), self._stream), "pq3d_aca_batched")
+                ranks = d_rank.cpu().numpy()
+                flags = d_flag.cpu().numpy()
+                keep = {}
+                for j, (ti, wo, kmax) in enumerate(batch):
+                    if flags[j] & 1 and kmax < min(tasks[ti]["m"], tasks[ti]["n"]):
+                        tasks[ti]["kcap"] = min(2 * kmax, min(tasks[ti]["m"], tasks[ti]["n"]))
+                        retry.append(ti)
+                        continue
+                    self.aca_ranks[ti] = ranks[j]
+                    self.aca_flags[ti] = flags[j]
+                    keep[ti] = (wo, kmax)
+                self.aca_ws.append((ws, keep))
+            pending = retry
+        self.task_ws = {}
+        for wi, (ws, keep) in enumerate(self.aca_ws):
+            for ti, (wo, kmax) in keep.items():
+                self.task_ws[ti] = (wi, wo, kmax)
+
+    def ranks(self):
+        """(kS, kD) per ACA block."""
+        r = self.aca_ranks.reshape(-1, 2)
+        return r[:, 0], r[:, 1]
+
+    # ------------------------------------------------------------------ packing / plans
+    def plan(self, dtype):
+        if dtype in self.plans:
+            return self.plans[dtype]
+        torch = self.torch
+        code = DTYPES[dtype]
+        cwd, cwl = _CW_DENSE[code], _CW_LR[code]
+        n = self.n
+        # dense items (column chunks x 32-row groups); slots per (block, chunk)
+        recs = self.dense_recs
+        ditems, slot_rows = [], []   # slot_rows: (slot_base, r0, m)
+        slot = 0
+        dense_off = recs["off64"] if code == 0 else recs["off32"]
+        for i in range(len(recs)):
+            m, nn, r0, c0 = int(recs["m"][i]), int(recs["n"][i]), int(recs["r0"][i]), int(recs["c0"][i])
+            ng = _cdiv(nn, cwd)
+            for g0 in range(0, ng, self.DENSE_CHUNK_GROUPS):
+                g1 = min(ng, g0 + self.DENSE_CHUNK_GROUPS)
+                for r in range(0, m, 32):
+                    ditems.append((int(dense_off[i]), m, r, g0, g1, c0, slot))
+                slot_rows.append((slot, r0, m))
+                slot += m
+        # low-rank blocks
+        kS, kD = self.ranks()
+        lr = []
+        u_off = v_off = 0
+        tp = 0
+        tb = 0
+        vitems, uitems, tblocks, pack = [], [], [], []
+        for bi, b in enumerate(self.aca_blocks):
+            m, nn = len(b.row.indices), len(b.col.indices)
+            ks, kd = int(kS[bi]), int(kD[bi])
+            if ks + kd == 0:
+                continue
+            K = _cdiv(ks + kd, cwl) * cwl
+            Q = 3 * (ks + kd)
+            ngv = _cdiv(nn, cwl)
+            nch = _cdiv(ngv, self.V_CHUNK_GROUPS)
+            for ch in range(nch):
+                g0 = ch * self.V_CHUNK_GROUPS
+                g1 = min(ngv, g0 + self.V_CHUNK_GROUPS)
+                for q in range(0, Q, 32):
+                    vitems.append((v_off, Q, q, g0, g1, b.col.start, ks, tp + ch * Q))
+            tblocks.append((ks, kd, K, Q, tp, nch, tb, 0))
+            for r in range(0, m, 32):
+                uitems.append((u_off, m, r, K, ks, kd, slot, tb, nch))
+            slot_rows.append((slot, b.row.start, m))
+            for p in (0, 1):
+                ti = 2 * bi + p
+                wi, wo, kmax = self.task_ws[ti]
+                pack.append((wi, (wo, u_off, v_off, int(ro) if False else 0, 0, m, nn, kmax, ks if p == 0 else kd, p,
+                                  ks, kd, K, Q, b.row.start, b.col.start, 1 if self.aca_flags[ti] & 2 else 0), bi))
+            slot += m
+            tp += nch * Q
+            tb += 3 * K
+            u_off += _cdiv(K, cwl) * m * 3 * cwl
+            v_off += ngv * Q * cwl
+        lr_dtype = torch.float64 if code == 0 else (torch.float32 if code == 1 else torch.bfloat16)
+        Ubuf = torch.zeros(max(u_off, 8), dtype=lr_dtype, device=self.dev)
+        Vbuf = torch.zeros(max(v_off, 8), dtype=lr_dtype, device=self.dev)
+        # pack per workspace
+        ro_np = self._row_offsets()
+        for wi, (ws, _) in enumerate(self.aca_ws):
+            sel = [p for p in pack if p[0] == wi]
+            if not sel:
+                continue
+            rec = np.zeros(len(sel), dtype=_lib.PACK_TASK)
+            for j, (_, tup, bi) in enumerate(sel):
+                tup = list(tup)
+                tup[3] = ro_np[bi][0]
+                tup[4] = ro_np[bi][1]
+                rec[j] = tuple(tup)
+            d_rec = torch.from_numpy(rec.view(np.uint8)).to(self.dev)
+            check(self.L.pq3d_aca_pack(ptr(d_rec), len(sel), ptr(ws), ptr(self.rowlist), ptr(self.collist),
+                                       ptr(self.iperm), code, ptr(Ubuf), ptr(Vbuf), self._stream), "pq3d_aca_pack")
+        # per-leaf slot lists: slot index of row i = off + i
+        nleaf = len(self.s.leaves)
+        leaf_start = np.array([lf.start for lf in self.s.leaves], dtype=np.int64)
+        leaf_of_row = np.empty(n, dtype=np.int32)
+        for lf in self.s.leaves:
+            leaf_of_row[lf.start:lf.start + len(lf.indices)] = lf.leaf_id
+        sr = np.array(slot_rows, dtype=np.int64).reshape(-1, 3)
+        first = leaf_of_row[sr[:, 1]]
+        last = leaf_of_row[sr[:, 1] + sr[:, 2] - 1]
+        cnt = (last - first + 1).astype(np.int64)
+        rep_leaf = np.repeat(first, cnt) + (np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt))
+        rep_off = np.repeat(sr[:, 0] - sr[:, 1], cnt)
+        order = np.argsort(rep_leaf, kind="stable")
+        leaf_off = rep_off[order].astype(np.int32)
+        leaf_ptr = np.zeros(nleaf + 1, dtype=np.int32)
+        np.add.at(leaf_ptr, rep_leaf + 1, 1)
+        leaf_ptr = np.cumsum(leaf_ptr).astype(np.int32)
+        del leaf_start
+
+        def dev_rec(rows, dt):
+            a = np.array(rows, dtype=dt) if rows else np.zeros(1, dtype=dt)
+            return torch.from_numpy(a.view(np.uint8)).to(self.dev), len(rows)
+
+        d_ditems, nd = dev_rec(ditems, _lib.DENSE_ITEM)
+        d_vitems, nv = dev_rec(vitems, _lib.V_ITEM)
+        d_uitems, nu = dev_rec(uitems, _lib.U_ITEM)
+        d_tblocks, nt = dev_rec(tblocks, _lib.T_BLOCK)
+        acc = torch.float64 if code == 0 else torch.float32
+        P = dict(code=code, dtype=dtype, acc=acc,
+                 dense=self.dense64 if code == 0 else self.dense32, U=Ubuf, V=Vbuf,
+                 ditems=d_ditems, vitems=d_vitems, uitems=d_uitems, tblocks=d_tblocks,
+                 leaf_of_row=torch.tensor(leaf_of_row, device=self.dev),
+                 leaf_ptr=torch.tensor(leaf_ptr, device=self.dev),
+                 leaf_off=torch.tensor(leaf_off if len(leaf_off) else np.zeros(1, np.int32), device=self.dev),
+                 n_ditems=nd, n_vitems=nv, n_uitems=nu, n_lr=nt, n_slots=slot, n_tpart=tp, n_t=tb)
+        P["slots"] = torch.empty(3 * max(slot, 1), dtype=acc, device=self.dev)
+        P["tpart"] = torch.empty(max(tp, 1), dtype=acc, device=self.dev)
+        P["t"] = torch.empty(max(tb, 1), dtype=acc, device=self.dev)
+        hp = np.zeros(1, dtype=_lib.HM_PLAN)
+        hp["n"] = n
+        hp["dtype"] = code
+        for k in ("dense", "U", "V", "ditems", "vitems", "uitems", "tblocks", "leaf_of_row", "leaf_ptr", "leaf_off"):
+            hp[k] = P[k].data_ptr() if P[k] is not None else 0
+        for k in ("n_ditems", "n_vitems", "n_uitems", "n_lr", "n_slots", "n_tpart", "n_t"):
+            hp[k] = P[k]
+        P["host_plan"] = hp
+        # algorithmic bytes of one application (operator data + x + y)
+        esz_d = 8 if code == 0 else 4
+        esz_l = {0: 8, 1: 4, 2: 2}[code]
+        dense_entries = int(np.sum(recs["m"].astype(np.int64) * recs["n"])) if len(recs) else 0
+        lr_entries = 0
+        for bi, b in enumerate(self.aca_blocks):
+            m, nn = len(b.row.indices), len(b.col.indices)
+            lr_entries += 3 * (int(kS[bi]) + int(kD[bi])) * (m + nn)
+        P["alg_bytes"] = dense_entries * 6 * esz_d + lr_entries * esz_l + 2 * n * esz_d + 3 * n * 8
+        P["stored_bytes"] = (P["dense"].numel() * P["dense"].element_size() if P["dense"] is not None else 0) + \
+            Ubuf.numel() * Ubuf.element_size() + Vbuf.numel() * Vbuf.element_size()
+        self.plans[dtype] = P
+        return P
+
+    def _row_offsets(self):
+        if not hasattr(self, "_ro_cache"):
+            ro, co = 0, 0
+            res = []
+            for b in self.aca_blocks:
+                res.append((ro, co))
+                ro += len(b.row.indices)
+                co += len(b.col.indices)
+            self._ro_cache = res
+        return self._ro_cache
+
+    def new_x(self, dtype):
+        """Zero interleaved deficit buffer (tree order) with padding for the given plan."""
+        P = self.plan(dtype)
+        return self.torch.zeros(2 * (self.n + 16), dtype=P["acc"], device=self.dev)
+
+    def matvec(self, x, dtype, y=None, add=(None, None, None), stream=None):
+        """y[i, c] = sum_j K_c(i, j) x  (tree order, FP64 output)."""
+        P = self.plan(dtype)
+        if y is None:
+            y = self.torch.empty((self.n, 3), dtype=self.torch.float64, device=self.dev)
+        st = _lib.stream_ptr(stream)
+        check(self.L.pq3d_hmatvec(P["host_plan"].ctypes.data, ptr(x), ptr(P["slots"]), ptr(P["tpart"]), ptr(P["t"]),
+                                  ptr(add[0]), ptr(add[1]), ptr(add[2]), ptr(y), st), "pq3d_hmatvec")
+        return y
+
+    def apply(self, x1, x2, dtype="fp64"):
+        """Host convenience: (y1, y2, yB) in element order for deficits x1, x2 (element order)."""
+        torch = self.torch
+        P = self.plan(dtype)
+        xt = np.zeros(2 * (self.n + 16))
+        xt[0:2 * self.n:2] = np.asarray(x1)[self.s.perm]
+        xt[1:2 * self.n:2] = np.asarray(x2)[self.s.perm]
+        x = torch.tensor(xt, dtype=P["acc"], device=self.dev)
+        y = self.matvec(x, dtype).cpu().numpy()
+        out = np.empty_like(y)
+        out[self.s.perm] = y
+        return out[:, 0], out[:, 1], out[:, 2]
+
+
+def export_blocks(op):
+    """Host copy of the FP64 operator per block, in the reference's block format:
+    list of ("dense", rows, cols, M[6][m][n]) or ("aca", rows, cols, S, D) with
+    S/D dicts of U1 V1 U2 V2 UB VB (rows/cols are element ids in tree order).
+    Used to run the reference's CPU step on the same operator."""
+    P = op.plan("fp64")
+    perm = op.s.perm
+    dense = op.dense64.cpu().numpy() if op.dense64 is not None else None
+    U = P["U"].cpu().numpy()
+    V = P["V"].cpu().numpy()
+    out = []
+    recs = op.dense_recs
+    for i in range(len(recs)):
+        m, n, r0, c0 = (int(recs[k][i]) for k in ("m", "n", "r0", "c0"))
+        ng = _cdiv(n, 2)
+        a = dense[int(recs["off64"][i]):int(recs["off64"][i]) + ng * m * 12].reshape(ng, m, 3, 2, 2)
+        # (group, row, comp, slip, t) -> (slip, comp, row, col)
+        M = a.transpose(3, 2, 1, 0, 4).reshape(2, 3, m, ng * 2)[:, :, :, :n].reshape(6, m, n)
+        out.append(("dense", perm[r0:r0 + m], perm[c0:c0 + n], np.ascontiguousarray(M)))
+    kS, kD = op.ranks()
+    u_off = v_off = 0
+    for bi, b in enumerate(op.aca_blocks):
+        m, n = len(b.row.indices), len(b.col.indices)
+        ks, kd = int(kS[bi]), int(kD[bi])
+        rows = perm[b.row.start:b.row.start + m]
+        cols = perm[b.col.start:b.col.start + n]
+        if ks + kd == 0:
+            z = dict(U1=np.zeros((m, 0)), V1=np.zeros((0, n)), U2=np.zeros((m, 0)), V2=np.zeros((0, n)), UB=[], VB=[])
+            out.append(("aca", rows, cols, z, dict(z)))
+            continue
+        K = _cdiv(ks + kd, 2) * 2
+        Q = 3 * (ks + kd)
+        ngv = _cdiv(n, 2)
+        Ub = U[u_off:u_off + K // 2 * m * 6].reshape(K // 2, m, 3, 2).transpose(2, 1, 0, 3).reshape(3, m, K)
+        Vb = V[v_off:v_off + ngv * Q * 2].reshape(ngv, Q, 2).transpose(1, 0, 2).reshape(Q, ngv * 2)[:, :n]
+        S, D = {}, {}
+        for c, (un, vn) in enumerate((("U1", "V1"), ("U2", "V2"), ("UB", "VB"))):
+            S[un] = np.ascontiguousarray(Ub[c, :, :ks])
+            S[vn] = np.ascontiguousarray(Vb[c * ks:(c + 1) * ks])
+            D[un] = np.ascontiguousarray(Ub[c, :, ks:ks + kd])
+            D[vn] = np.ascontiguousarray(Vb[3 * ks + c * kd:3 * ks + (c + 1) * kd])
+        out.append(("aca", rows, cols, S, D))
+        u_off += K // 2 * m * 6
+        v_off += ngv * Q * 2
+    return out

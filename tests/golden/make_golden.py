@@ -1,0 +1,259 @@
+"""Generate the golden fixtures in tests/golden/ by running the REFERENCE itself.
+
+Run in a container that has the reference tree (default /root/reference):
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+What it does:
+  * builds the reference's TDstressFS_C.cpp from source (oracle/Makefile, target
+    `ref`) -- the shipped binary is never used;
+  * imports the reference's Python modules (src/readmsh.py, src/QDsim.py,
+    src/Hmatrix.py, src/SH_greenfunction.py) with single-rank stand-ins for
+    mpi4py and no-op stand-ins for matplotlib and pyvista (plotting and VTK
+    reading are off the hot path), from a scratch directory holding
+    src/TDstressFS_C.so, the relative path Hmatrix.py loads;
+  * records reference outputs:
+      gf_cases.npz      stress/strain of TDstressFS_C and TDstressEachSourceAtReceiver_C
+                        (full and half space) on fixed and random receivers,
+                        including on-plane, on-edge and vertex points, plus
+                        the numpy twin SH_greenfunction.TDstressFS
+      tiny_case.npz     a 576-element jittered planar fault: frames, initial
+                        state, block structure, ACA ranks and factors of
+                        a few blocks, the six operator products on fixed
+                        vectors, and 30 simu_forward steps (seeded ACA starts)
+The fixtures are small (< 1 MB) and are what the CPU tests pin against.
+"""
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+
+def install_stubs():
+    class Comm:
+        def Get_rank(self):
+            return 0
+
+        def Get_size(self):
+            return 1
+
+        def bcast(self, x, root=0):
+            return x
+
+        def reduce(self, x, op=None, root=0):
+            return x
+
+        def Barrier(self):
+            pass
+
+    mpi = types.ModuleType("mpi4py.MPI")
+    mpi.COMM_WORLD = Comm()
+    mpi.SUM = "sum"
+    mpi.Wtime = __import__("time").time
+    pkg = types.ModuleType("mpi4py")
+    pkg.MPI = mpi
+    sys.modules["mpi4py"] = pkg
+    sys.modules["mpi4py.MPI"] = mpi
+
+    class Anything(types.ModuleType):
+        def __getattr__(self, name):
+            return lambda *a, **k: None
+
+    mpl = Anything("matplotlib")
+    plt = Anything("matplotlib.pyplot")
+    plt.rcParams = {}
+    cols = Anything("matplotlib.colors")
+    mpl.pyplot = plt
+    mpl.colors = cols
+    sys.modules["matplotlib"] = mpl
+    sys.modules["matplotlib.pyplot"] = plt
+    sys.modules["matplotlib.colors"] = cols
+    sys.modules["pyvista"] = Anything("pyvista")
+
+
+def gf_cases(lib, SH):
+    import ctypes
+    D = ctypes.POINTER(ctypes.c_double)
+    lib.TDstressFS_C.argtypes = [D, D, D, ctypes.c_size_t, D, D, D] + [ctypes.c_double] * 5 + [ctypes.c_bool, D, D]
+    lib.TDstressEachSourceAtReceiver_C.argtypes = [ctypes.c_double] * 3 + [D, D, D, ctypes.c_size_t] + \
+        [ctypes.c_double] * 5 + [ctypes.c_bool, D, D]
+    p = lambda a: a.ctypes.data_as(D)
+    out = {}
+    # (1) the fixed inputs of the reference's own main() (src/TDstressFS_C.cpp:2004-2023)
+    X = np.array([48771.61733949, -48484.78117283, 48775.26818703])
+    Y = np.array([30000., 15000., 3000.])
+    Z = np.array([-13944.10291502, -20994.9909562, -12042.91174556])
+    P1 = np.array([-49019.8529842, 0., -13632.75018015])
+    P2 = np.array([-49294.4187163, 3000., -14516.85867197])
+    P3 = np.array([-48427.27119853, 0., -14642.195744633])
+    mu = lam = 32038120320.0
+    for hs in (False, True):
+        s, e = np.zeros(18), np.zeros(18)
+        lib.TDstressFS_C(p(X), p(Y), p(Z), 3, p(P1), p(P2), p(P3), 1.0, 0.5, 0.0, mu, lam, hs, p(s), p(e))
+        out["main_%s_stress" % ("hs" if hs else "fs")] = s.reshape(3, 6)
+        out["main_%s_strain" % ("hs" if hs else "fs")] = e.reshape(3, 6)
+    out["main_X"], out["main_Y"], out["main_Z"] = X, Y, Z
+    out["main_P"] = np.stack([P1, P2, P3])
+    # (2) random triangles and receivers, with special points
+    rng = np.random.default_rng(1234)
+    tris, recs = [], []
+    for t in range(12):
+        c = np.array([rng.uniform(-5e3, 5e3), rng.uniform(-5e3, 5e3), rng.uniform(-20e3, -8e3)])
+        P = c + rng.normal(size=(3, 3)) * 1500.0
+        if t == 11:   # vertical triangle
+            P[:, 1] = c[1]
+        R = c + rng.normal(size=(160, 3)) * 4000.0
+        Rz = R.copy()
+        # special receivers: vertices, edge midpoints, centroid, on-plane outside points
+        cen = P.mean(axis=0)
+        mids = [(P[0] + P[1]) / 2, (P[1] + P[2]) / 2, (P[2] + P[0]) / 2]
+        extra = [P[0], P[1], P[2], cen] + mids + [cen + 2.5 * (P[0] - cen), cen + 2.5 * (mids[1] - cen),
+                                                   2 * P[1] - P[0], cen + 1e-3 * np.cross(P[1] - P[0], P[2] - P[0])]
+        R = np.concatenate([Rz, np.array(extra)])
+        tris.append(P)
+        recs.append(R)
+    tris = np.array(tris)
+    recs = np.array(recs)
+    out["rand_P"], out["rand_R"] = tris, recs
+    for Ss, Ds, tag in ((1.0, 0.0, "ss"), (0.0, 1.0, "ds"), (0.7, -0.4, "mix")):
+        S = np.zeros(recs.shape[:2] + (6,))
+        E = np.zeros_like(S)
+        SH_S = np.zeros_like(S)
+        for t in range(len(tris)):
+            R = np.ascontiguousarray(recs[t])
+            n = len(R)
+            s, e = np.zeros(6 * n), np.zeros(6 * n)
+            x, y, z = (np.ascontiguousarray(R[:, k]) for k in range(3))
+            lib.TDstressFS_C(p(x), p(y), p(z), n, p(tris[t, 0].copy()), p(tris[t, 1].copy()), p(tris[t, 2].copy()),
+                             Ss, Ds, 0.0, mu, lam, False, p(s), p(e))
+            S[t], E[t] = s.reshape(n, 6), e.reshape(n, 6)
+            st, _ = SH.TDstressFS(x.copy(), y.copy(), z.copy(), tris[t, 0].copy(), tris[t, 1].copy(),
+                                  tris[t, 2].copy(), Ss, Ds, 0.0, mu, lam)
+            SH_S[t] = np.asarray(st).T
+        out["rand_%s_stress" % tag], out["rand_%s_strain" % tag], out["rand_%s_numpy" % tag] = S, E, SH_S
+    # (3) one receiver, many sources (TDstressEachSourceAtReceiver_C)
+    r = recs[0, 5]
+    n = len(tris)
+    P1f, P2f, P3f = (np.ascontiguousarray(tris[:, k].ravel()) for k in range(3))
+    s, e = np.zeros(6 * n), np.zeros(6 * n)
+    lib.TDstressEachSourceAtReceiver_C(r[0], r[1], r[2], p(P1f), p(P2f), p(P3f), n, 1.0, 0.0, 0.0, mu, lam, False,
+                                       p(s), p(e))
+    out["each_R"], out["each_stress"], out["each_strain"] = r, s.reshape(n, 6), e.reshape(n, 6)
+    out["mu"], out["lam"] = mu, lam
+    return out
+
+
+def tiny_case(workdir, QDsim_mod, readmsh, Hmatrix):
+    sys.path.insert(0, REPO)
+    from pyquake3d_b200 import meshgen
+    msh, para = meshgen.make_case("tiny", os.path.join(workdir, "tiny"), n_target=600)
+    nodes, tris = readmsh.read_mshV2(msh)
+    sim = QDsim_mod.QDsim(tris, nodes, para)
+    out = {"nodes": nodes, "tris": tris, "eleVec": sim.eleVec, "xg": sim.xg}
+    for k in ("Tno", "Tt1o", "Tt2o", "state", "slipv1", "slipv2", "slipv", "a", "b", "dc", "f0", "rake",
+              "shear_loading", "normal_loading", "slipvC", "Tt", "fric"):
+        out["init_" + k] = np.array(getattr(sim, k), dtype=np.float64)
+    tb = sim.tree_block
+    tb.blocks_to_process = []
+    tb.collect_blocks(tb.root_block)
+    blocks = tb.blocks_to_process
+    rc = [np.asarray(b.row_cluster) for b in blocks]
+    cc = [np.asarray(b.col_cluster) for b in blocks]
+    out["blk_m"] = np.array([len(r) for r in rc])
+    out["blk_n"] = np.array([len(c) for c in cc])
+    out["blk_rows"] = np.concatenate(rc)
+    out["blk_cols"] = np.concatenate(cc)
+    SEED = 7
+    np.random.seed(SEED)
+    for b in blocks:
+        tb.ACA_worker(b)
+    out["aca_seed"] = SEED
+    out["blk_aca"] = np.array([bool(b.judaca) for b in blocks])
+    ks, kd, fac = [], [], {}
+    na = 0
+    for i, b in enumerate(blocks):
+        if b.judaca:
+            ks.append(b.ACA_dictS["U_ACA_A1s"].shape[1])
+            kd.append(b.ACA_dictD["U_ACA_A1d"].shape[1])
+            if na < 3:
+                for key in ("U_ACA_A1s", "V_ACA_A1s", "U_ACA_A2s", "V_ACA_A2s", "U_ACA_Bs", "V_ACA_Bs"):
+                    fac["f%d_%s" % (i, key)] = np.asarray(b.ACA_dictS[key], dtype=np.float64)
+                for key in ("U_ACA_A1d", "V_ACA_A1d", "U_ACA_A2d", "V_ACA_A2d", "U_ACA_Bd", "V_ACA_Bd"):
+                    fac["f%d_%s" % (i, key)] = np.asarray(b.ACA_dictD[key], dtype=np.float64)
+                na += 1
+    out["aca_kS"], out["aca_kD"] = np.array(ks), np.array(kd)
+    out.update(fac)
+    # operator products on fixed vectors
+    rng = np.random.default_rng(99)
+    X = rng.standard_normal((2, len(sim.xg))) * 1e-9
+    out["mvm_x"] = X
+    for op in ("A1s", "A2s", "Bs", "A1d", "A2d", "Bd"):
+        x = X[0] if op.endswith("s") else X[1]
+        out["mvm_" + op] = tb.blocks_process_MVM(x, blocks, op)
+    # time stepping
+    sim.local_blocks = blocks
+    hs, dts, ts = [], [], []
+    dttry = sim.htry
+    snaps = {}
+    for i in range(30):
+        h, dtnext = sim.simu_forward(dttry)
+        hs.append(h)
+        dts.append(dtnext)
+        ts.append(sim.time)
+        dttry = dtnext
+        if i in (0, 29):
+            for k in ("Tno", "Tt1o", "Tt2o", "state", "slipv1", "slipv2", "slipv", "slip1", "slip2", "slip", "rake"):
+                snaps["step%d_%s" % (i + 1, k)] = np.array(getattr(sim, k), dtype=np.float64)
+    out["steps_h"], out["steps_dtnext"], out["steps_time"] = np.array(hs), np.array(dts), np.array(ts)
+    out.update(snaps)
+    with open(para) as f:
+        out["parameter_txt"] = np.array(f.read())
+    with open(os.path.join(os.path.dirname(para), "tinyparam.dat")) as f:
+        out["param_dat"] = np.array(f.read())
+    with open(msh) as f:
+        out["msh"] = np.array(f.read())
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    args = ap.parse_args()
+    ref_src = os.path.join(args.ref, "src")
+    subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref", "REFSRC=" + os.path.join(ref_src, "TDstressFS_C.cpp")],
+                   check=True)
+    work = tempfile.mkdtemp(prefix="pq3d_golden_")
+    os.makedirs(os.path.join(work, "src"))
+    shutil.copy(os.path.join(REPO, "oracle", "_ref", "TDstressFS_C.so"), os.path.join(work, "src", "TDstressFS_C.so"))
+    install_stubs()
+    sys.path.insert(0, ref_src)
+    cwd = os.getcwd()
+    os.chdir(work)
+    try:
+        import ctypes
+        import SH_greenfunction
+        import readmsh
+        import Hmatrix
+        import QDsim
+        lib = ctypes.CDLL(os.path.join(work, "src", "TDstressFS_C.so"))
+        g = gf_cases(lib, SH_greenfunction)
+        np.savez_compressed(os.path.join(HERE, "gf_cases.npz"), **g)
+        t = tiny_case(work, QDsim, readmsh, Hmatrix)
+        np.savez_compressed(os.path.join(HERE, "tiny_case.npz"), **t)
+    finally:
+        os.chdir(cwd)
+        shutil.rmtree(work, ignore_errors=True)
+    for f in ("gf_cases.npz", "tiny_case.npz"):
+        print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
+
+
+if __name__ == "__main__":
+    main()

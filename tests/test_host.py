@@ -1,0 +1,62 @@
+"""Host logic against the reference run on the tiny case: mesh reading, element
+frames, initial conditions and the H-matrix block structure."""
+import numpy as np
+
+from pyquake3d_b200 import read_mshV2, get_eleVec
+from pyquake3d_b200.hmatrix import HStructure, aca_start_indices
+
+
+def test_mesh_and_frames(tiny_files, tiny_golden):
+    g = tiny_golden
+    nodes, tris = read_mshV2(tiny_files[0])
+    assert np.array_equal(nodes, g["nodes"])
+    assert np.array_equal(tris, g["tris"])
+    ev, xg = get_eleVec(nodes, tris, False)
+    assert np.array_equal(ev, g["eleVec"])
+    assert np.array_equal(xg, g["xg"])
+
+
+def test_initial_conditions(tiny_sim, tiny_golden):
+    g = tiny_golden
+    for k in ("Tno", "Tt1o", "Tt2o", "state", "slipv1", "slipv2", "slipv", "a", "b", "dc", "f0", "rake",
+              "shear_loading", "normal_loading", "slipvC", "Tt", "fric"):
+        assert np.array_equal(getattr(tiny_sim, k), g["init_" + k]), k
+
+
+def test_block_structure_matches_reference(tiny_sim, tiny_golden):
+    g = tiny_golden
+    blocks = tiny_sim.tree_block.struct.blocks
+    assert len(blocks) == len(g["blk_m"])
+    ro = np.concatenate([[0], np.cumsum(g["blk_m"])])
+    co = np.concatenate([[0], np.cumsum(g["blk_n"])])
+    for i, b in enumerate(blocks):
+        assert np.array_equal(b.row.indices, g["blk_rows"][ro[i]:ro[i + 1]])
+        assert np.array_equal(b.col.indices, g["blk_cols"][co[i]:co[i + 1]])
+        assert b.aca == bool(g["blk_aca"][i])
+
+
+def test_tree_order_ranges(tiny_sim):
+    s = tiny_sim.tree_block.struct
+    assert np.array_equal(np.sort(s.perm), np.arange(s.n))
+    for b in s.blocks:
+        assert np.array_equal(np.sort(s.perm[b.row.start:b.row.start + len(b.row.indices)]), b.row.indices)
+        assert np.array_equal(np.sort(s.perm[b.col.start:b.col.start + len(b.col.indices)]), b.col.indices)
+
+
+def test_blocks_cover_matrix_once(tiny_sim):
+    s = tiny_sim.tree_block.struct
+    cover = np.zeros((s.n, s.n), dtype=np.int32)
+    for b in s.blocks:
+        cover[np.ix_(b.row.indices, b.col.indices)] += 1
+    assert (cover == 1).all()
+
+
+def test_seeded_aca_starts_match_reference_draws(tiny_sim, tiny_golden):
+    """np.random.seed(s) + the reference's randint calls == aca_start_indices(blocks, s)."""
+    blocks = tiny_sim.tree_block.struct.blocks
+    st = aca_start_indices(blocks, int(tiny_golden["aca_seed"]))
+    np.random.seed(int(tiny_golden["aca_seed"]))
+    for b, (s, d) in zip([b for b in blocks if b.aca], st):
+        m, n = len(b.row.indices), len(b.col.indices)
+        assert s == (np.random.randint(m) - 3, np.random.randint(n) - 3)
+        assert d == (np.random.randint(m) - 3, np.random.randint(n) - 3)
