@@ -191,6 +191,103 @@ def aca_start_indices(blocks, seed):
     return out
 
 
+# ----------------------------------------------------------------------------- packed layout (host)
+
+
+def dense_layout(dense_blocks):
+    """DenseBlock records with FP64 / FP32 offsets, and the two array sizes."""
+    recs = np.zeros(len(dense_blocks), dtype=_lib.DENSE_BLOCK)
+    off64 = off32 = 0
+    for i, b in enumerate(dense_blocks):
+        m, n = len(b.row.indices), len(b.col.indices)
+        recs[i] = (off64, off32, m, n, b.row.start, b.col.start)
+        off64 += _cdiv(n, 2) * m * 12
+        off32 += _cdiv(n, 4) * m * 24
+    return recs, off64, off32
+
+
+def build_plan_arrays(struct, dense_recs, kS, kD, code, dense_chunk=64, v_chunk=64):
+    """Matvec work items, slot layout and per-leaf slot lists for storage code
+    (0 FP64, 1 FP32, 2 FP32 dense + BF16 low rank).  Pure numpy.
+
+    Slots: every dense (block, column chunk) and every low-rank block owns m
+    consecutive slots (one per block row); row i of a block with slot base s
+    and first row r0 writes slot s + (i - r0).  leaf_off lists, per leaf
+    cluster, the offsets s - r0 of all slot owners covering that leaf."""
+    cwd, cwl = _CW_DENSE[code], _CW_LR[code]
+    n = struct.n
+    ditems, slot_rows = [], []
+    slot = 0
+    dense_off = dense_recs["off64"] if code == 0 else dense_recs["off32"]
+    for i in range(len(dense_recs)):
+        m, nn, r0, c0 = (int(dense_recs[k][i]) for k in ("m", "n", "r0", "c0"))
+        ng = _cdiv(nn, cwd)
+        for g0 in range(0, ng, dense_chunk):
+            g1 = min(ng, g0 + dense_chunk)
+            for r in range(0, m, 32):
+                ditems.append((int(dense_off[i]), m, r, g0, g1, c0, slot))
+            slot_rows.append((slot, r0, m))
+            slot += m
+    aca_blocks = [b for b in struct.blocks if b.aca]
+    u_off = v_off = tp = tb = 0
+    vitems, uitems, tblocks, pack = [], [], [], []
+    lr_entries = 0
+    for bi, b in enumerate(aca_blocks):
+        m, nn = len(b.row.indices), len(b.col.indices)
+        ks, kd = int(kS[bi]), int(kD[bi])
+        lr_entries += 3 * (ks + kd) * (m + nn)
+        if ks + kd == 0:
+            continue
+        K = _cdiv(ks + kd, cwl) * cwl
+        Q = 3 * (ks + kd)
+        ngv = _cdiv(nn, cwl)
+        nch = _cdiv(ngv, v_chunk)
+        for ch in range(nch):
+            g0 = ch * v_chunk
+            g1 = min(ngv, g0 + v_chunk)
+            for q in range(0, Q, 32):
+                vitems.append((v_off, Q, q, g0, g1, b.col.start, ks, tp + ch * Q))
+        tblocks.append((ks, kd, K, Q, tp, nch, tb, 0))
+        for r in range(0, m, 32):
+            uitems.append((u_off, m, r, K, ks, kd, slot, tb, nch))
+        slot_rows.append((slot, b.row.start, m))
+        for p in (0, 1):
+            pack.append((bi, p, u_off, v_off, K, Q, ks, kd))
+        slot += m
+        tp += nch * Q
+        tb += 3 * K
+        u_off += (K // cwl) * m * 3 * cwl
+        v_off += ngv * Q * cwl
+    nleaf = len(struct.leaves)
+    leaf_of_row = np.empty(n, dtype=np.int32)
+    for lf in struct.leaves:
+        leaf_of_row[lf.start:lf.start + len(lf.indices)] = lf.leaf_id
+    sr = np.array(slot_rows, dtype=np.int64).reshape(-1, 3)
+    first = leaf_of_row[sr[:, 1]].astype(np.int64)
+    last = leaf_of_row[sr[:, 1] + sr[:, 2] - 1].astype(np.int64)
+    cnt = last - first + 1
+    rep_leaf = np.repeat(first, cnt) + (np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt))
+    rep_off = np.repeat(sr[:, 0] - sr[:, 1], cnt)
+    order = np.argsort(rep_leaf, kind="stable")
+    leaf_off = rep_off[order].astype(np.int32)
+    leaf_ptr = np.zeros(nleaf + 1, dtype=np.int64)
+    np.add.at(leaf_ptr, rep_leaf + 1, 1)
+    leaf_ptr = np.cumsum(leaf_ptr).astype(np.int32)
+
+    def rec(rows, dt):
+        return np.array(rows, dtype=dt) if rows else np.zeros(1, dtype=dt)
+
+    esz_d = 8 if code == 0 else 4
+    esz_l = {0: 8, 1: 4, 2: 2}[code]
+    dense_entries = int(np.sum(dense_recs["m"].astype(np.int64) * dense_recs["n"])) if len(dense_recs) else 0
+    return dict(ditems=rec(ditems, _lib.DENSE_ITEM), vitems=rec(vitems, _lib.V_ITEM), uitems=rec(uitems, _lib.U_ITEM),
+                tblocks=rec(tblocks, _lib.T_BLOCK), n_ditems=len(ditems), n_vitems=len(vitems),
+                n_uitems=len(uitems), n_lr=len(tblocks), n_slots=slot, n_tpart=tp, n_t=tb,
+                u_size=u_off, v_size=v_off, pack=pack, leaf_of_row=leaf_of_row, leaf_ptr=leaf_ptr,
+                leaf_off=leaf_off if len(leaf_off) else np.zeros(1, np.int32), slot_rows=sr,
+                alg_bytes=dense_entries * 6 * esz_d + lr_entries * esz_l + 2 * n * esz_d + 3 * n * 8)
+
+
 # ----------------------------------------------------------------------------- device operator
 
 DTYPES = {"fp64": 0, "fp32": 1, "bf16": 2}
@@ -269,13 +366,7 @@ class DeviceHMatrix:
         torch = self.torch
         need64 = "fp64" in want
         need32 = any(d in want for d in ("fp32", "bf16"))
-        recs = np.zeros(len(self.dense_blocks), dtype=_lib.DENSE_BLOCK)
-        off64 = off32 = 0
-        for i, b in enumerate(self.dense_blocks):
-            m, n = len(b.row.indices), len(b.col.indices)
-            recs[i] = (off64, off32, m, n, b.row.start, b.col.start)
-            off64 += _cdiv(n, 2) * m * 12
-            off32 += _cdiv(n, 4) * m * 24
+        recs, off64, off32 = dense_layout(self.dense_blocks)
         order = np.argsort(-(recs["m"].astype(np.int64) * recs["n"]), kind="stable")
         self.dense_recs = recs
         self.dense64 = torch.zeros(max(off64, 1), dtype=torch.float64, device=self.dev) if need64 else None
@@ -377,130 +468,53 @@ class DeviceHMatrix:
             return self.plans[dtype]
         torch = self.torch
         code = DTYPES[dtype]
-        cwd, cwl = _CW_DENSE[code], _CW_LR[code]
-        n = self.n
-        # dense items (column chunks x 32-row groups); slots per (block, chunk)
-        recs = self.dense_recs
-        ditems, slot_rows = [], []   # slot_rows: (slot_base, r0, m)
-        slot = 0
-        dense_off = recs["off64"] if code == 0 else recs["off32"]
-        for i in range(len(recs)):
-            m, nn, r0, c0 = int(recs["m"][i]), int(recs["n"][i]), int(recs["r0"][i]), int(recs["c0"][i])
-            ng = _cdiv(nn, cwd)
-            for g0 in range(0, ng, self.DENSE_CHUNK_GROUPS):
-                g1 = min(ng, g0 + self.DENSE_CHUNK_GROUPS)
-                for r in range(0, m, 32):
-                    ditems.append((int(dense_off[i]), m, r, g0, g1, c0, slot))
-                slot_rows.append((slot, r0, m))
-                slot += m
-        # low-rank blocks
         kS, kD = self.ranks()
-        lr = []
-        u_off = v_off = 0
-        tp = 0
-        tb = 0
-        vitems, uitems, tblocks, pack = [], [], [], []
-        for bi, b in enumerate(self.aca_blocks):
-            m, nn = len(b.row.indices), len(b.col.indices)
-            ks, kd = int(kS[bi]), int(kD[bi])
-            if ks + kd == 0:
-                continue
-            K = _cdiv(ks + kd, cwl) * cwl
-            Q = 3 * (ks + kd)
-            ngv = _cdiv(nn, cwl)
-            nch = _cdiv(ngv, self.V_CHUNK_GROUPS)
-            for ch in range(nch):
-                g0 = ch * self.V_CHUNK_GROUPS
-                g1 = min(ngv, g0 + self.V_CHUNK_GROUPS)
-                for q in range(0, Q, 32):
-                    vitems.append((v_off, Q, q, g0, g1, b.col.start, ks, tp + ch * Q))
-            tblocks.append((ks, kd, K, Q, tp, nch, tb, 0))
-            for r in range(0, m, 32):
-                uitems.append((u_off, m, r, K, ks, kd, slot, tb, nch))
-            slot_rows.append((slot, b.row.start, m))
-            for p in (0, 1):
-                ti = 2 * bi + p
-                wi, wo, kmax = self.task_ws[ti]
-                pack.append((wi, (wo, u_off, v_off, int(ro) if False else 0, 0, m, nn, kmax, ks if p == 0 else kd, p,
-                                  ks, kd, K, Q, b.row.start, b.col.start, 1 if self.aca_flags[ti] & 2 else 0), bi))
-            slot += m
-            tp += nch * Q
-            tb += 3 * K
-            u_off += _cdiv(K, cwl) * m * 3 * cwl
-            v_off += ngv * Q * cwl
+        A = build_plan_arrays(self.s, self.dense_recs, kS, kD, code, self.DENSE_CHUNK_GROUPS, self.V_CHUNK_GROUPS)
         lr_dtype = torch.float64 if code == 0 else (torch.float32 if code == 1 else torch.bfloat16)
-        Ubuf = torch.zeros(max(u_off, 8), dtype=lr_dtype, device=self.dev)
-        Vbuf = torch.zeros(max(v_off, 8), dtype=lr_dtype, device=self.dev)
-        # pack per workspace
+        Ubuf = torch.zeros(max(A["u_size"], 8), dtype=lr_dtype, device=self.dev)
+        Vbuf = torch.zeros(max(A["v_size"], 8), dtype=lr_dtype, device=self.dev)
+        # pack every ACA task into the layout, one launch per workspace batch
         ro_np = self._row_offsets()
-        for wi, (ws, _) in enumerate(self.aca_ws):
-            sel = [p for p in pack if p[0] == wi]
-            if not sel:
-                continue
-            rec = np.zeros(len(sel), dtype=_lib.PACK_TASK)
-            for j, (_, tup, bi) in enumerate(sel):
-                tup = list(tup)
-                tup[3] = ro_np[bi][0]
-                tup[4] = ro_np[bi][1]
-                rec[j] = tuple(tup)
+        by_ws = {}
+        for (bi, p, u_off, v_off, K, Q, ks, kd) in A["pack"]:
+            ti = 2 * bi + p
+            wi, wo, kmax = self.task_ws[ti]
+            b = self.aca_blocks[bi]
+            by_ws.setdefault(wi, []).append((wo, u_off, v_off, ro_np[bi][0], ro_np[bi][1], len(b.row.indices),
+                                             len(b.col.indices), kmax, ks if p == 0 else kd, p, ks, kd, K, Q,
+                                             b.row.start, b.col.start, 1 if self.aca_flags[ti] & 2 else 0))
+        for wi, rows in by_ws.items():
+            rec = np.array(rows, dtype=_lib.PACK_TASK)
             d_rec = torch.from_numpy(rec.view(np.uint8)).to(self.dev)
-            check(self.L.pq3d_aca_pack(ptr(d_rec), len(sel), ptr(ws), ptr(self.rowlist), ptr(self.collist),
-                                       ptr(self.iperm), code, ptr(Ubuf), ptr(Vbuf), self._stream), "pq3d_aca_pack")
-        # per-leaf slot lists: slot index of row i = off + i
-        nleaf = len(self.s.leaves)
-        leaf_start = np.array([lf.start for lf in self.s.leaves], dtype=np.int64)
-        leaf_of_row = np.empty(n, dtype=np.int32)
-        for lf in self.s.leaves:
-            leaf_of_row[lf.start:lf.start + len(lf.indices)] = lf.leaf_id
-        sr = np.array(slot_rows, dtype=np.int64).reshape(-1, 3)
-        first = leaf_of_row[sr[:, 1]]
-        last = leaf_of_row[sr[:, 1] + sr[:, 2] - 1]
-        cnt = (last - first + 1).astype(np.int64)
-        rep_leaf = np.repeat(first, cnt) + (np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt))
-        rep_off = np.repeat(sr[:, 0] - sr[:, 1], cnt)
-        order = np.argsort(rep_leaf, kind="stable")
-        leaf_off = rep_off[order].astype(np.int32)
-        leaf_ptr = np.zeros(nleaf + 1, dtype=np.int32)
-        np.add.at(leaf_ptr, rep_leaf + 1, 1)
-        leaf_ptr = np.cumsum(leaf_ptr).astype(np.int32)
-        del leaf_start
+            check(self.L.pq3d_aca_pack(ptr(d_rec), len(rows), ptr(self.aca_ws[wi][0]), ptr(self.rowlist),
+                                       ptr(self.collist), ptr(self.iperm), code, ptr(Ubuf), ptr(Vbuf), self._stream),
+                  "pq3d_aca_pack")
 
-        def dev_rec(rows, dt):
-            a = np.array(rows, dtype=dt) if rows else np.zeros(1, dtype=dt)
-            return torch.from_numpy(a.view(np.uint8)).to(self.dev), len(rows)
+        def dev_rec(a):
+            return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8)).to(self.dev)
 
-        d_ditems, nd = dev_rec(ditems, _lib.DENSE_ITEM)
-        d_vitems, nv = dev_rec(vitems, _lib.V_ITEM)
-        d_uitems, nu = dev_rec(uitems, _lib.U_ITEM)
-        d_tblocks, nt = dev_rec(tblocks, _lib.T_BLOCK)
         acc = torch.float64 if code == 0 else torch.float32
         P = dict(code=code, dtype=dtype, acc=acc,
                  dense=self.dense64 if code == 0 else self.dense32, U=Ubuf, V=Vbuf,
-                 ditems=d_ditems, vitems=d_vitems, uitems=d_uitems, tblocks=d_tblocks,
-                 leaf_of_row=torch.tensor(leaf_of_row, device=self.dev),
-                 leaf_ptr=torch.tensor(leaf_ptr, device=self.dev),
-                 leaf_off=torch.tensor(leaf_off if len(leaf_off) else np.zeros(1, np.int32), device=self.dev),
-                 n_ditems=nd, n_vitems=nv, n_uitems=nu, n_lr=nt, n_slots=slot, n_tpart=tp, n_t=tb)
-        P["slots"] = torch.empty(3 * max(slot, 1), dtype=acc, device=self.dev)
-        P["tpart"] = torch.empty(max(tp, 1), dtype=acc, device=self.dev)
-        P["t"] = torch.empty(max(tb, 1), dtype=acc, device=self.dev)
+                 ditems=dev_rec(A["ditems"]), vitems=dev_rec(A["vitems"]), uitems=dev_rec(A["uitems"]),
+                 tblocks=dev_rec(A["tblocks"]),
+                 leaf_of_row=torch.tensor(A["leaf_of_row"], device=self.dev),
+                 leaf_ptr=torch.tensor(A["leaf_ptr"], device=self.dev),
+                 leaf_off=torch.tensor(A["leaf_off"], device=self.dev),
+                 n_ditems=A["n_ditems"], n_vitems=A["n_vitems"], n_uitems=A["n_uitems"], n_lr=A["n_lr"],
+                 n_slots=A["n_slots"], n_tpart=A["n_tpart"], n_t=A["n_t"])
+        P["slots"] = torch.empty(3 * max(P["n_slots"], 1), dtype=acc, device=self.dev)
+        P["tpart"] = torch.empty(max(P["n_tpart"], 1), dtype=acc, device=self.dev)
+        P["t"] = torch.empty(max(P["n_t"], 1), dtype=acc, device=self.dev)
         hp = np.zeros(1, dtype=_lib.HM_PLAN)
-        hp["n"] = n
+        hp["n"] = self.n
         hp["dtype"] = code
         for k in ("dense", "U", "V", "ditems", "vitems", "uitems", "tblocks", "leaf_of_row", "leaf_ptr", "leaf_off"):
             hp[k] = P[k].data_ptr() if P[k] is not None else 0
         for k in ("n_ditems", "n_vitems", "n_uitems", "n_lr", "n_slots", "n_tpart", "n_t"):
             hp[k] = P[k]
         P["host_plan"] = hp
-        # algorithmic bytes of one application (operator data + x + y)
-        esz_d = 8 if code == 0 else 4
-        esz_l = {0: 8, 1: 4, 2: 2}[code]
-        dense_entries = int(np.sum(recs["m"].astype(np.int64) * recs["n"])) if len(recs) else 0
-        lr_entries = 0
-        for bi, b in enumerate(self.aca_blocks):
-            m, nn = len(b.row.indices), len(b.col.indices)
-            lr_entries += 3 * (int(kS[bi]) + int(kD[bi])) * (m + nn)
-        P["alg_bytes"] = dense_entries * 6 * esz_d + lr_entries * esz_l + 2 * n * esz_d + 3 * n * 8
+        P["alg_bytes"] = A["alg_bytes"]
         P["stored_bytes"] = (P["dense"].numel() * P["dense"].element_size() if P["dense"] is not None else 0) + \
             Ubuf.numel() * Ubuf.element_size() + Vbuf.numel() * Vbuf.element_size()
         self.plans[dtype] = P
