@@ -138,6 +138,19 @@ int pq3d_rk_grid(int n);
  * [9] total rejects, [10] total attempts. */
 int pq3d_rk_step(const void *args, int grid, cudaStream_t stream);
 
+/* No counterpart in the reference.  The same step as pq3d_rk_step for callers
+ * that cannot allocate device memory (a host framework that owns every device
+ * buffer, an embedded solver handed only its state vectors, a time loop that
+ * must not call cudaMalloc).  The scratch of args (cand, blk, bar) is ignored:
+ * the step uses a static array inside libpq3d.so (about 4.5 MB, held by every
+ * GPU that loads the library until exit).  Limits: n <= 131072 elements and
+ * grid <= 4096 CTAs; larger sizes return PQ3D_ERR_NOMEM without launching.
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture.  All calls share the array (its barrier counter
+ * is cleared on the stream before each launch), so calls that overlap on the
+ * GPU race.  Allocates nothing. */
+int pq3d_rk_step_noalloc(const void *args, int grid, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -328,3 +328,83 @@ PQ3D_EXPORT int pq3d_rk_step(const void *args, int grid, cudaStream_t stream)
     PQ3D_CHECK(cudaLaunchKernelEx(&cfg, k_rk_step, A));
     return PQ3D_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of pq3d_rk_step.
+//
+// Some callers cannot allocate device memory: code that runs inside another
+// framework's memory pool or under a host-side allocation policy, embedded
+// solvers that only receive pre-allocated state vectors, and callers that
+// must not call cudaMalloc in their time loop.  For them the step's scratch
+// (candidate state, per-CTA error maxima, grid-barrier counter) lives in the
+// file-scope array below, reserved in device memory when the library is
+// loaded and held by every GPU that loads it until the process exits.
+// Limits: n <= PQ3D_NOALLOC_MAX_N elements and grid <= PQ3D_NOALLOC_MAX_GRID
+// CTAs (about 4.5 MB per device).  All calls share the array: the barrier
+// counter is cleared on the stream before each launch, and calls that overlap
+// on the GPU (different streams, or several threads) race on it.
+#define PQ3D_NOALLOC_MAX_N 131072
+#define PQ3D_NOALLOC_MAX_GRID 4096
+
+static __device__ __align__(256) double g_rk_scratch[4 * PQ3D_NOALLOC_MAX_N + 10 * PQ3D_NOALLOC_MAX_GRID + 2];
+
+#include <mutex>
+#include <stdio.h>
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+double *g_scratch_dev[kMaxDevices] = {nullptr};
+
+// Device address of g_rk_scratch on the current device.  The name is only a
+// host-side stand-in, so the address is looked up once per device (with that
+// device current) and cached.
+int scratch_address(double **out)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PQ3D_ERR_CUDA;
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (!g_scratch_dev[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_rk_scratch) != cudaSuccess || !p) return PQ3D_ERR_CUDA;
+        g_scratch_dev[dev] = (double *)p;
+    }
+    *out = g_scratch_dev[dev];
+    return PQ3D_OK;
+}
+}  // namespace
+
+// Same step as pq3d_rk_step; the cand, blk and bar members of args are ignored.
+// The first call on a device looks up the scratch address (make that call
+// before any stream capture).  Allocates nothing.
+PQ3D_EXPORT int pq3d_rk_step_noalloc(const void *args, int grid, cudaStream_t stream)
+{
+    if (!args || grid <= 0) return PQ3D_ERR_ARG;
+    RkArgs A = *(const RkArgs *)args;
+    if (A.n <= 0 || !A.ctrl || !A.y || !A.x) return PQ3D_ERR_ARG;
+    if (A.n > PQ3D_NOALLOC_MAX_N || grid > PQ3D_NOALLOC_MAX_GRID) {
+        fprintf(stderr, "pq3d_rk_step_noalloc: n=%d, grid=%d exceed the static scratch (n <= %d, grid <= %d)\n",
+                A.n, grid, PQ3D_NOALLOC_MAX_N, PQ3D_NOALLOC_MAX_GRID);
+        return PQ3D_ERR_NOMEM;
+    }
+    double *s = nullptr;
+    int rc = scratch_address(&s);
+    if (rc != PQ3D_OK) return rc;
+    A.cand = s;
+    A.blk = s + 4 * (size_t)PQ3D_NOALLOC_MAX_N;
+    A.bar = (unsigned *)(s + 4 * (size_t)PQ3D_NOALLOC_MAX_N + 10 * (size_t)PQ3D_NOALLOC_MAX_GRID);
+    // the barrier counter must start at zero; the rest is written before it is read
+    PQ3D_CHECK(cudaMemsetAsync(A.bar, 0, 2 * sizeof(unsigned), stream));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    PQ3D_CHECK(cudaLaunchKernelEx(&cfg, k_rk_step, A));
+    return PQ3D_OK;
+}
