@@ -46,6 +46,11 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def set_case(name):
+    global CASE
+    CASE = name
+
+
 def make_case(rank=0):
     from pyquake3d_b200 import meshgen
     d = os.path.join(tempfile.gettempdir(), "pq3d_bench_%s_r%d" % (CASE, rank))
@@ -110,6 +115,51 @@ def cpu_reference_steps(ho, state, V0, mu, Cs, budget_s, max_steps=20):
             break
     dt = time.perf_counter() - t0
     return k / dt, k, dt
+
+
+def accuracy_study(sim, op, nrep, precisions=("bf16",), marks=(50, 100, 200, 500)):
+    """Relative L2 errors of slip, V and psi of each precision against the FP64 operator
+    at equal times (dt replay of the FP64 run), after each mark; plus the FP64 chaos
+    floor: the same errors between two FP64 runs whose initial shear tractions differ by a
+    relative 1e-12."""
+    import torch
+    from pyquake3d_b200.qdsim import DeviceStepper
+
+    def errs(a, b):
+        sa = torch.sqrt(a.t["slip1"] ** 2 + a.t["slip2"] ** 2)
+        sb = torch.sqrt(b.t["slip1"] ** 2 + b.t["slip2"] ** 2)
+        r = lambda u, v: float(torch.linalg.norm(u - v) / torch.linalg.norm(v))
+        return {"slip": r(sa, sb), "V": r(a.t["slipv"], b.t["slipv"]), "psi": r(a.t["psi"], b.t["psi"])}
+
+    marks = [m for m in marks if m <= nrep] or [nrep]
+    ref = DeviceStepper(sim, op, "fp64")
+    others = {p: DeviceStepper(sim, op, p) for p in precisions if p in op.plans}
+    pert = DeviceStepper(sim, op, "fp64")
+    pert.t["Tt1o"].mul_(1.0 + 1e-12)
+    for st in [ref, pert] + list(others.values()):
+        st.ctrl[0] = sim.htry
+    ref.set_history(nrep)
+    out = {p: [] for p in others}
+    out["fp64_perturbed_1e-12"] = []
+    done = 0
+    for mk in marks:
+        for i in range(done, mk):
+            ref.launch(i)
+        torch.cuda.synchronize()
+        h = ref.hist.view(-1, 6)[:, 0]
+        for name, st in list(others.items()) + [("fp64_perturbed_1e-12", pert)]:
+            st.set_replay(h)
+            for i in range(done, mk):
+                st.launch(i)
+        torch.cuda.synchronize()
+        for name, st in list(others.items()) + [("fp64_perturbed_1e-12", pert)]:
+            e = errs(st, ref)
+            e["steps"] = mk
+            out[name].append(e)
+        done = mk
+    out["method"] = "dt replay of the FP64 run; relative L2 over elements"
+    out["sim_time_s"] = float(ref.hist.view(-1, 6)[done - 1, 2])
+    return out
 
 
 # --------------------------------------------------------------------- reference arm (CPU)
@@ -188,8 +238,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--case", default=CASE, help="workload (profiling uses a smaller one)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    set_case(args.case)
 
     import torch
     import torch.distributed as dist
@@ -213,6 +265,7 @@ def main():
     nodes, tris = read_mshV2(msh)
     t0 = time.perf_counter()
     sim = QDsim(tris, nodes, para, device="cuda:%d" % local, precision="bf16")
+    sim.tree_block.want = ("fp64", "bf16", "fp32")
     t_host = time.perf_counter() - t0
     op = sim.tree_block.op()
     t_asm = time.perf_counter() - t0 - t_host
@@ -232,15 +285,30 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def timed_steps(stepper, k, dttry):
-        stepper.set_history(k)
+    graphs = {}
+
+    def timed_steps(stepper, k, dttry, use_graph=True):
+        """k steps; with use_graph, replays of a captured graph of G steps (k multiple of G)."""
+        G = 100
+        g = None
+        if use_graph and k % G == 0 and k >= G:
+            key = id(stepper)
+            if key not in graphs:
+                graphs[key] = stepper.capture(G)
+            g = graphs[key]
+        if g is None:
+            stepper.set_history(k)
         stepper.ctrl[0] = dttry
         barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for i in range(k):
-            stepper.launch(i)
+        if g is not None:
+            for _ in range(k // G):
+                g.replay()
+        else:
+            for i in range(k):
+                stepper.launch(i)
         e1.record()
         torch.cuda.synchronize()
         barrier()
@@ -251,13 +319,14 @@ def main():
 
     # warm-up (both paths), then the timed mixed-precision region with clock sampling
     dt_m = dt_p = sim.htry
-    _, dt_m = timed_steps(mixed, args.warmup, dt_m)
-    _, dt_p = timed_steps(plain, args.warmup, dt_p)
+    _, dt_m = timed_steps(mixed, args.warmup, dt_m, use_graph=False)
+    _, dt_p = timed_steps(plain, args.warmup, dt_p, use_graph=False)
     clk = Clocks(local)
     t_mixed, dt_m = timed_steps(mixed, args.steps, dt_m)
     clocks = clk.stop()
     t_mixed = max_over_ranks(t_mixed)
-    hist_m = mixed.hist.view(-1, 6).cpu().numpy()[:args.steps]
+    hist_m = mixed.hist.view(-1, 6).cpu().numpy()[:min(args.steps, mixed.hist_cap)]
+    graph_used = id(mixed) in graphs and graphs[id(mixed)] is not None
     t_plain, dt_p = timed_steps(plain, args.steps, dt_p)
     t_plain = max_over_ranks(t_plain)
     steps_total = args.steps * world
@@ -265,13 +334,15 @@ def main():
 
     # H-matvec alone (the dominant kernel sequence), CUDA events on the launching stream
     def time_matvec(stepper, P, reps=50):
+        # the operator application as the step runs it (dense/V and U launches; the
+        # per-row sums are folded into the step kernel)
         for _ in range(5):
-            op.matvec(stepper.x, stepper.precision, y=stepper.y)
+            op.matvec(stepper.x, stepper.precision, slots_only=True)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(reps):
-            op.matvec(stepper.x, stepper.precision, y=stepper.y)
+            op.matvec(stepper.x, stepper.precision, slots_only=True)
         e1.record()
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / 1e3 / reps
@@ -281,26 +352,9 @@ def main():
     gbs_m = P_m["alg_bytes"] / t_mv_m / 1e9
     gbs_p = P_p["alg_bytes"] / t_mv_p / 1e9
 
-    # slip error of the mixed path vs the FP64 path at equal times (dt replay)
-    rep_p = DeviceStepper(sim, op, "fp64")
-    rep_m = DeviceStepper(sim, op, "bf16")
-    nrep = min(args.steps, 500)
-    rep_p.set_history(nrep)
-    rep_p.ctrl[0] = sim.htry
-    for i in range(nrep):
-        rep_p.launch(i)
-    rep_m.set_replay(rep_p.hist.view(-1, 6)[:, 0])
-    rep_m.ctrl[0] = sim.htry
-    for i in range(nrep):
-        rep_m.launch(i)
-    torch.cuda.synchronize()
-    s_p = torch.sqrt(rep_p.t["slip1"] ** 2 + rep_p.t["slip2"] ** 2)
-    s_m = torch.sqrt(rep_m.t["slip1"] ** 2 + rep_m.t["slip2"] ** 2)
-    slip_err = float(torch.linalg.norm(s_m - s_p) / torch.linalg.norm(s_p))
-    v_err = float(torch.linalg.norm(rep_m.t["slipv"] - rep_p.t["slipv"]) / torch.linalg.norm(rep_p.t["slipv"]))
-    th_p = rep_p.t["psi"]
-    th_err = float(torch.linalg.norm(rep_m.t["psi"] - th_p) / torch.linalg.norm(th_p))
-    del rep_p, rep_m
+    # accuracy vs the FP64 path at equal times (dt replay of the FP64 run), at several horizons
+    accuracy = accuracy_study(sim, op, min(args.steps, 500), precisions=("bf16", "fp32"))
+    slip_err = accuracy["bf16"][-1]["slip"]
 
     # end to end through the reference call surface (QDsim.simu_forward) with the
     # reference main loop's per-step host traffic
@@ -346,7 +400,7 @@ def main():
             traffic = json.load(open(tp)).get("bytes_per_matvec_bf16")
         except (ValueError, OSError):
             traffic = None
-    nlaunch_step = (4 if P_m["n_lr"] > 0 else 2) + 1
+    nlaunch_step = (2 if P_m["n_utasks"] > 0 else 1) + 1
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed / args.steps, "higher_is_better": True,
@@ -361,19 +415,19 @@ def main():
                    "parallelism": "replicas x%d" % world, "host_setup_s": round(t_host, 2),
                    "assembly_s": round(t_asm, 2), "assembly_breakdown": {k: round(v, 3) for k, v in op.timings.items()}},
         "roofline": {"bound": "hbm", "achieved": gbs_m, "peak": hbm, "unit": "GB/s", "frac": gbs_m / hbm,
-                     "traffic": traffic, "kernel": "H-matvec (4 launches), bf16/fp32",
+                     "traffic": traffic, "kernel": "H-matvec (k_dense_v + k_u), bf16 low rank / fp32 near field",
                      "alg_bytes": int(P_m["alg_bytes"]), "ms": 1e3 * t_mv_m, "peak_source": peak_kind},
         "plain_fp64": {"steps_per_s": steps_total / t_plain, "ms_per_step": 1e3 * t_plain / args.steps,
                        "hmatvec_GBs": gbs_p, "hmatvec_ms": 1e3 * t_mv_p, "alg_bytes": int(P_p["alg_bytes"]),
                        "frac": gbs_p / hbm},
         "mixed_vs_plain": (steps_total / t_mixed) / (steps_total / t_plain),
-        "accuracy_vs_fp64": {"slip_rel_l2": slip_err, "V_rel_l2": v_err, "psi_rel_l2": th_err,
-                             "steps": nrep, "method": "dt replay of the FP64 run"},
+        "accuracy_vs_fp64": accuracy,
         "sim": {"time_s": float(hist_m[-1, 2]), "last_dt": float(hist_m[-1, 0]),
                 "rejects": int(hist_m[:, 5].sum())},
         "e2e": e2e,
         "cpu_baseline": cpu,
         "gpu_launches": nlaunch_step * args.steps,
+        "cuda_graph": graph_used,
         "clocks": clocks,
     }
     if rank == 0:

@@ -114,16 +114,18 @@ int pq3d_aca_pack(const void *d_tasks, int64_t n_tasks, const double *d_ws,
 
 /* ---------------------------------------------------------------- H-matvec */
 
-/* Sizes of the work-item records: kind 0 DenseItem, 1 VItem, 2 UItem, 3 TBlock,
+/* Sizes of the work-item records: kind 0 DenseItem, 1 VItem, 2 UTask,
  * 4 DenseBlock, 5 the plan struct. */
 size_t pq3d_item_bytes(int kind);
 
 /* y (n x 3, FP64) = [A1s A1d; A2s A2d; Bs Bd] x (+ add0/add1/add2 per component).
  * Replaces the six BlockTree.blocks_process_MVM calls of QDsim.simu_forward
  * (src/Hmatrix.py:1445-1538, src/QDsim.py:906-917).  plan_host is a host copy of
- * the plan (device pointers inside); x interleaved strike/dip deficit. */
+ * the plan (device pointers inside); x interleaved strike/dip deficit.  d_y may be
+ * NULL: then only the per-row partial sums (d_slots) are written, for the step
+ * kernel to reduce. */
 int pq3d_hmatvec(const void *plan_host, const void *d_x, void *d_slots, void *d_tpart,
-                 void *d_t, const double *d_add0, const double *d_add1,
+                 const double *d_add0, const double *d_add1,
                  const double *d_add2, double *d_y, cudaStream_t stream);
 
 /* ---------------------------------------------------------------- stepper */

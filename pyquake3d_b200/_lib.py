@@ -19,22 +19,22 @@ i32 = ctypes.c_int
 # Record layouts (must match pyquake3d_b200/csrc/*.cu; checked at load time).
 DENSE_BLOCK = np.dtype([("off64", "i8"), ("off32", "i8"), ("m", "i4"), ("n", "i4"), ("r0", "i4"), ("c0", "i4")], align=True)
 DENSE_ITEM = np.dtype([("off", "i8"), ("m", "i4"), ("r", "i4"), ("g0", "i4"), ("g1", "i4"), ("c0", "i4"), ("slot", "i4")], align=True)
-V_ITEM = np.dtype([("off", "i8"), ("Q", "i4"), ("q", "i4"), ("g0", "i4"), ("g1", "i4"), ("c0", "i4"), ("kS", "i4"), ("tp", "i4")], align=True)
-U_ITEM = np.dtype([("off", "i8"), ("m", "i4"), ("r", "i4"), ("K", "i4"), ("kS", "i4"), ("kD", "i4"), ("slot", "i4"), ("tp", "i4"), ("nch", "i4")], align=True)
-T_BLOCK = np.dtype([("kS", "i4"), ("kD", "i4"), ("K", "i4"), ("Q", "i4"), ("tp", "i4"), ("nch", "i4"), ("tb", "i4"), ("pad", "i4")], align=True)
+V_ITEM = np.dtype([("off", "i8"), ("Q", "i4"), ("q", "i4"), ("nr", "i4"), ("g0", "i4"), ("g1", "i4"), ("c0", "i4"), ("s", "i4"), ("tp", "i4")], align=True)
+U_TASK = np.dtype([("off", "i8"), ("m", "i4"), ("r0", "i4"), ("r1", "i4"), ("K", "i4"), ("kS", "i4"), ("kD", "i4"), ("Q", "i4"), ("tp", "i4"), ("nch", "i4"), ("slot", "i4")], align=True)
 ACA_TASK = np.dtype([("rows_off", "i8"), ("cols_off", "i8"), ("ws_off", "i8"), ("m", "i4"), ("n", "i4"), ("kmax", "i4"), ("pass_", "i4"), ("iref0", "i4"), ("jref0", "i4")], align=True)
 PACK_TASK = np.dtype([("ws_off", "i8"), ("u_off", "i8"), ("v_off", "i8"), ("rows_off", "i8"), ("cols_off", "i8"),
                       ("m", "i4"), ("n", "i4"), ("kmax", "i4"), ("k", "i4"), ("pass_", "i4"), ("kS", "i4"), ("kD", "i4"),
                       ("K", "i4"), ("Q", "i4"), ("r0", "i4"), ("c0", "i4"), ("zeroB", "i4")], align=True)
-_PLAN_PTRS = ["dense", "U", "V", "ditems", "vitems", "uitems", "tblocks", "leaf_of_row", "leaf_ptr", "leaf_off"]
+_PLAN_PTRS = ["dense", "U", "V", "ditems", "vitems", "utasks", "leaf_of_row", "leaf_ptr", "leaf_off"]
 HM_PLAN = np.dtype([("n", "i4"), ("dtype", "i4")] + [(p, "u8") for p in _PLAN_PTRS] +
-                   [(k, "i8") for k in ("n_ditems", "n_vitems", "n_uitems", "n_lr", "n_slots", "n_tpart", "n_t")], align=True)
+                   [(k, "i8") for k in ("n_ditems", "n_vitems", "n_utasks", "n_slots", "n_tpart")] +
+                   [("kmax", "i4"), ("pad", "i4")], align=True)
 _RK_PTRS = ["Tno", "Tt1o", "Tt2o", "psi", "slip1", "slip2", "slipv1", "slipv2", "slipv", "rake", "Tt", "fric", "slip",
             "a", "b", "dc", "f0", "shear_loading", "normal_loading", "vplc", "cr0", "sr0",
-            "y", "cand", "blk", "x", "ctrl", "hist", "hforce", "bar"]
+            "y", "cand", "blk", "x", "ctrl", "hist", "hforce", "bar", "slots", "leaf_of_row", "leaf_ptr", "leaf_off"]
 RK_ARGS = np.dtype([(p, "u8") for p in _RK_PTRS] +
-                   [("n", "i4"), ("fix_tn", "i4"), ("x_fp32", "i4"), ("step_index", "i4"),
-                    ("V0", "f8"), ("eta", "f8"), ("reltol", "f8")], align=True)
+                   [("n", "i4"), ("fix_tn", "i4"), ("x_fp32", "i4"), ("step_index", "i4"), ("fuse_rowsum", "i4"),
+                    ("slots_fp32", "i4"), ("V0", "f8"), ("eta", "f8"), ("reltol", "f8")], align=True)
 
 _lib = None
 
@@ -83,17 +83,15 @@ def load():
     L.pq3d_aca_pack.argtypes = [vp, i64, vp, vp, vp, vp, i32, vp, vp, vp]
     L.pq3d_item_bytes.argtypes = [i32]
     L.pq3d_item_bytes.restype = ctypes.c_size_t
-    L.pq3d_hmatvec.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.pq3d_hmatvec.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.pq3d_rk_args_bytes.restype = ctypes.c_size_t
     L.pq3d_rk_grid.argtypes = [i32]
     L.pq3d_rk_step.argtypes = [vp, i32, vp]
-    for name in [n for n in dir(L) if n.startswith("pq3d_")]:
-        pass
     for f in ("pq3d_src_records", "pq3d_traction_pairs", "pq3d_stress_points", "pq3d_dense_assemble",
               "pq3d_aca_batched", "pq3d_aca_pack", "pq3d_hmatvec", "pq3d_rk_grid", "pq3d_rk_step"):
         getattr(L, f).restype = ctypes.c_int
     sizes = {"DenseItem": (L.pq3d_item_bytes(0), DENSE_ITEM.itemsize), "VItem": (L.pq3d_item_bytes(1), V_ITEM.itemsize),
-             "UItem": (L.pq3d_item_bytes(2), U_ITEM.itemsize), "TBlock": (L.pq3d_item_bytes(3), T_BLOCK.itemsize),
+             "UTask": (L.pq3d_item_bytes(2), U_TASK.itemsize),
              "DenseBlock": (L.pq3d_item_bytes(4), DENSE_BLOCK.itemsize), "HmPlan": (L.pq3d_item_bytes(5), HM_PLAN.itemsize),
              "AcaTask": (L.pq3d_aca_task_bytes(), ACA_TASK.itemsize), "PackTask": (L.pq3d_pack_task_bytes(), PACK_TASK.itemsize),
              "RkArgs": (L.pq3d_rk_args_bytes(), RK_ARGS.itemsize)}

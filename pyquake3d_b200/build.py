@@ -12,9 +12,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpq3d.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 SOURCES = ["gf.cu", "aca.cu", "hmatvec.cu", "rk.cu"]
-# The stepper is compiled without FMA contraction so its FP64 arithmetic rounds
-# like the reference's numpy expressions, operation by operation.
-EXTRA = {"rk.cu": ["-fmad=false"]}
+EXTRA = {}
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

@@ -441,7 +441,7 @@ __global__ void k_aca_pack(const PackTask *__restrict__ tasks, const double *__r
         double v = (c == 2 && P.zeroB) ? 0.0 : V[((int64_t)q * 3 + c) * P.n + j];
         int jt = iperm[cols[j]] - P.c0;
         int row = P.pass == 0 ? c * P.kS + q : 3 * P.kS + c * P.kD + q;
-        Vout[P.v_off + v_index(P.Q, row, jt, CW)] = cvt<T>(v);
+        Vout[P.v_off + v_index(P.Q, row, P.c0 % CW + jt, CW)] = cvt<T>(v);
     }
 }
 

@@ -245,8 +245,8 @@ __global__ void k_dense_assemble(const double *__restrict__ xg, const double *__
 #pragma unroll
             for (int comp = 0; comp < 3; ++comp) {
                 double v = t[3 * slip + comp];
-                if (out64) out64[B.off64 + dense_index(B.m, i, j, comp, slip, kCW64)] = v;
-                if (out32) out32[B.off32 + dense_index(B.m, i, j, comp, slip, kCW32)] = (float)v;
+                if (out64) out64[B.off64 + dense_index(B.m, i, j + B.c0 % kCW64, comp, slip, kCW64)] = v;
+                if (out32) out32[B.off32 + dense_index(B.m, i, j + B.c0 % kCW32, comp, slip, kCW32)] = (float)v;
             }
     }
 }

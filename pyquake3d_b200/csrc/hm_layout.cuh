@@ -4,8 +4,12 @@
 // left-first walk of the cluster tree), so every block covers contiguous
 // ranges [r0, r0+m) x [c0, c0+n) and the operator needs no gather/scatter.
 //
+// Column alignment: a block's stored columns start at the CW-aligned column
+// c0a = c0 - lead (lead = c0 % CW, zero-filled), so the x slice of a column group
+// is one aligned vector load.
+//
 // Dense block (m x n, six operators): element (row i, col j, comp c, slip s)
-//   at  ((j / CW) * m + i) * 6*CW + (2*c + s) * CW + (j % CW)
+//   at  ((jj / CW) * m + i) * 6*CW + (2*c + s) * CW + (jj % CW),  jj = j + lead
 // with comp c in {tau1, tau2, sigma_n} and slip s in {strike, dip}; CW is 4
 // for FP32 and 2 for FP64, so one row's CW columns for all six operators are
 // 96 contiguous bytes and 32 consecutive rows are 3 KB contiguous.
@@ -15,7 +19,14 @@
 //   t_c = [V_cs x_strike ; V_cd x_dip]
 // U element (row i, comp c, q) at ((q / CWU) * m + i) * 3*CWU + c*CWU + q % CWU.
 // V rows: Q = 3*kS + 3*kD rows (A1s, A2s, Bs rows first, then A1d, A2d, Bd),
-// element (row q, col j) at ((j / CWV) * Q + q) * CWV + j % CWV.
+// column-group major: element (q, j) at ((jj / CWV) * Q + q) * CWV + jj % CWV
+// with jj = lead + j, so 8 consecutive rows of one column group are 128
+// contiguous bytes.
+//
+// The deficit vector x (accumulation type) holds, with P = x_stride(n):
+//   x[0 .. 2P)    interleaved (strike, dip) per element  -- dense blocks
+//   x[2P .. 3P)   strike plane, x[3P .. 4P) dip plane     -- V rows
+// all zero beyond n.
 #pragma once
 #include <stdint.h>
 
@@ -39,23 +50,25 @@ __host__ __device__ inline int64_t u_index(int m, int i, int comp, int q, int cw
     return ((int64_t)(q / cwu) * m + i) * (3 * cwu) + comp * cwu + (q % cwu);
 }
 
-__host__ __device__ inline int64_t v_index(int Q, int q, int j, int cwv)
+__host__ __device__ inline int64_t v_index(int Q, int q, int jj, int cwv)
 {
-    return ((int64_t)(j / cwv) * Q + q) * cwv + (j % cwv);
+    return ((int64_t)(jj / cwv) * Q + q) * cwv + (jj % cwv);
 }
+
+__host__ __device__ inline int x_stride(int n) { return ((n + 16 + 7) / 8) * 8; }
 
 // Matvec work items (one warp each).
 struct DenseItem {          // rows [r, r+32) of a dense block, column groups [g0, g1)
     int64_t off;            // block offset in the dense array
     int32_t m, r, g0, g1, c0, slot;  // slot: slot index of block row 0 for this column chunk
 };
-struct VItem {              // V rows [q, q+32) of a low-rank block, column groups [g0, g1)
+struct VItem {              // V rows [q, q+nr) (nr <= 8, one slip) of a block, column groups [g0, g1)
     int64_t off;            // block offset in the V array
-    int32_t Q, q, g0, g1, c0, kS, tp;  // tp: offset of this chunk's partial t (Q values)
+    int32_t Q, q, nr, g0, g1, c0, s, tp;  // s: slip of these rows; tp: this chunk's partial t (Q values)
 };
-struct UItem {              // rows [r, r+32) of a low-rank block
+struct UTask {              // one CTA: rows [r0, r1) of a low-rank block
     int64_t off;            // block offset in the U array
-    int32_t m, r, K, kS, kD, slot, tp, nch;  // tp/nch: first chunk partial and chunk count (stride Q)
+    int32_t m, r0, r1, K, kS, kD, Q, tp, nch, slot;  // tp/nch: the block's chunk partials of t (stride Q)
 };
 
 }  // namespace pq3d

@@ -16,9 +16,10 @@
 //
 // Launch sequence (stream-ordered, no host sync):
 //   k_dense_v   dense items and V items (t partials = V x per column chunk)
-//   k_treduce   sum t partials per low-rank block -> t[block][3][K]
-//   k_u         U items: slot rows += U_c t_c
+//   k_u         per (low-rank block, row range): t from its chunk partials in
+//               shared memory, then slot rows = U_c t_c
 //   k_rowsum    y[i] = sum of row i's slots (FP64), plus optional loading terms
+//               (skipped when the step kernel sums the slots itself)
 #include "pq3d_common.cuh"
 #include "hm_layout.cuh"
 #include <cuda_bf16.h>
@@ -53,6 +54,18 @@ __device__ __forceinline__ Vec16<T> ld_stream(const T *p)
     return o;
 }
 
+// N values of T from an aligned address (N * sizeof(T) a multiple of 16), read-only path.
+template <typename T, int N>
+__device__ __forceinline__ void ld_vec(const T *p, T *o)
+{
+    static_assert((N * sizeof(T)) % 16 == 0, "16-byte multiples");
+#pragma unroll
+    for (int k = 0; k < (int)(N * sizeof(T) / 16); ++k) {
+        const int4 r = __ldg(reinterpret_cast<const int4 *>(p) + k);
+        memcpy(o + k * (16 / sizeof(T)), &r, 16);
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ float tof(T v);
 template <>
@@ -69,11 +82,13 @@ template <>
 __device__ __forceinline__ double widen<double, double>(double v) { return v; }
 
 // ------------------------------------------------------------------ kernel 1
+// Dense items (lanes over block rows) and V items (8 rows x 4 column groups per
+// warp load, then a 2-step shuffle reduction per row).
 template <typename TD, typename TL, typename TA>
 __global__ void __launch_bounds__(256)
 k_dense_v(const DenseItem *__restrict__ ditems, int64_t n_ditems, const VItem *__restrict__ vitems,
           int64_t n_vitems, const TD *__restrict__ D, const TL *__restrict__ Vd, const TA *__restrict__ x,
-          TA *__restrict__ slots, TA *__restrict__ tpart)
+          int xstride, TA *__restrict__ slots, TA *__restrict__ tpart)
 {
     constexpr int CWD = 16 / sizeof(TD);
     constexpr int CWV = 16 / sizeof(TL);
@@ -87,12 +102,11 @@ k_dense_v(const DenseItem *__restrict__ ditems, int64_t n_ditems, const VItem *_
         const TD *p = D + it.off + (int64_t)r * 6 * CWD;
         const int64_t gstride = (int64_t)it.m * 6 * CWD;
         p += (int64_t)it.g0 * gstride;
-        const TA *xp = x + 2 * ((int64_t)it.c0 + (int64_t)it.g0 * CWD);
+        const TA *xp = x + 2 * ((int64_t)it.c0 + (int64_t)it.g0 * CWD);   // c0 is CWD-aligned
 #pragma unroll 2
         for (int g = it.g0; g < it.g1; ++g) {
             TA xs[2 * CWD];
-#pragma unroll
-            for (int t = 0; t < 2 * CWD; ++t) xs[t] = xp[t];
+            ld_vec<TA, 2 * CWD>(xp, xs);
             if (act) {
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
@@ -116,82 +130,102 @@ k_dense_v(const DenseItem *__restrict__ ditems, int64_t n_ditems, const VItem *_
     const int64_t wv = w - n_ditems;
     if (wv >= n_vitems) return;
     const VItem it = vitems[wv];
-    const int q = it.q + lane;
-    if (q >= it.Q) return;
-    const int s = q < 3 * it.kS ? 0 : 1;
+    // lane = 8 * jg + rr: row q + rr, column groups g0 + jg, g0 + jg + 4, ...
+    const int rr = lane & 7, jg = lane >> 3;
     TA acc = 0;
-    const TL *p = Vd + it.off + ((int64_t)it.g0 * it.Q + q) * CWV;
-    const int64_t gstride = (int64_t)it.Q * CWV;
-    const TA *xp = x + 2 * ((int64_t)it.c0 + (int64_t)it.g0 * CWV) + s;
+    if (rr < it.nr) {
+        const TL *p = Vd + it.off + ((int64_t)(it.g0 + jg) * it.Q + it.q + rr) * CWV;
+        const int64_t gstride = (int64_t)4 * it.Q * CWV;
+        const TA *xp = x + (int64_t)(2 + it.s) * xstride + it.c0 + (int64_t)(it.g0 + jg) * CWV;  // CWV-aligned
 #pragma unroll 4
-    for (int g = it.g0; g < it.g1; ++g) {
-        Vec16<TL> d = ld_stream(p);
+        for (int g = it.g0 + jg; g < it.g1; g += 4) {
+            Vec16<TL> d = ld_stream(p);
+            TA xs[CWV];
+            ld_vec<TA, CWV>(xp, xs);
 #pragma unroll
-        for (int t = 0; t < CWV; ++t) acc += widen<TA>(d.v[t]) * xp[2 * t];
-        p += gstride;
-        xp += 2 * CWV;
+            for (int t = 0; t < CWV; ++t) acc += widen<TA>(d.v[t]) * xs[t];
+            p += gstride;
+            xp += 4 * CWV;
+        }
     }
-    tpart[it.tp + q] = acc;
+    acc += __shfl_xor_sync(0xffffffffu, acc, 8);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+    if (jg == 0 && rr < it.nr) tpart[it.tp + it.q + rr] = acc;
 }
 
 // ------------------------------------------------------------------ kernel 2
-// t[tb + c*K + q] = sum over chunks of the partial V x rows (zero in the K padding).
-struct TBlock {
-    int32_t kS, kD, K, Q, tp, nch, tb, pad;
-};
-
-template <typename TA>
-__global__ void k_treduce(const TBlock *__restrict__ tb, int64_t n_blocks, const TA *__restrict__ tpart,
-                          TA *__restrict__ t)
+// One CTA per (low-rank block, row range): sums the block's chunk partials of
+// t = V x into shared memory, then its warps stream U (lanes over rows).
+template <typename TA, int CW>
+__device__ __forceinline__ void smem_vec(const TA *p, TA *o)
 {
-    const int64_t b = blockIdx.x;
-    if (b >= n_blocks) return;
-    const TBlock B = tb[b];
-    for (int e = threadIdx.x; e < 3 * B.K; e += blockDim.x) {
-        const int c = e / B.K, q = e % B.K;
-        TA v = 0;
+#pragma unroll
+    for (int k = 0; k < CW; ++k) o[k] = p[k];
+}
+template <>
+__device__ __forceinline__ void smem_vec<float, 8>(const float *p, float *o)
+{
+    const float4 a = reinterpret_cast<const float4 *>(p)[0], b = reinterpret_cast<const float4 *>(p)[1];
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w; o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+}
+template <>
+__device__ __forceinline__ void smem_vec<float, 4>(const float *p, float *o)
+{
+    const float4 a = reinterpret_cast<const float4 *>(p)[0];
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+}
+template <>
+__device__ __forceinline__ void smem_vec<double, 2>(const double *p, double *o)
+{
+    const double2 a = reinterpret_cast<const double2 *>(p)[0];
+    o[0] = a.x; o[1] = a.y;
+}
+
+template <typename TL, typename TA>
+__global__ void __launch_bounds__(256)
+k_u(const UTask *__restrict__ tasks, const TL *__restrict__ U, const TA *__restrict__ tpart, TA *__restrict__ slots)
+{
+    constexpr int CW = 16 / sizeof(TL);
+    extern __shared__ __align__(16) unsigned char smraw[];
+    TA *ts = reinterpret_cast<TA *>(smraw);
+    const UTask T = tasks[blockIdx.x];
+    for (int e = threadIdx.x; e < 3 * T.K; e += blockDim.x) {
+        const int c = e / T.K, q = e % T.K;
         int row = -1;
-        if (q < B.kS) row = c * B.kS + q;
-        else if (q < B.kS + B.kD) row = 3 * B.kS + c * B.kD + (q - B.kS);
+        if (q < T.kS) row = c * T.kS + q;
+        else if (q < T.kS + T.kD) row = 3 * T.kS + c * T.kD + (q - T.kS);
+        TA v = 0;
         if (row >= 0)
-            for (int ch = 0; ch < B.nch; ++ch) v += tpart[B.tp + (int64_t)ch * B.Q + row];
-        t[B.tb + e] = v;
+            for (int ch = 0; ch < T.nch; ++ch) v += tpart[T.tp + (int64_t)ch * T.Q + row];
+        ts[e] = v;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ng = T.K / CW;
+    const int64_t gstride = (int64_t)T.m * 3 * CW;
+    for (int rb = T.r0 + warp * 32; rb < T.r1; rb += blockDim.x) {
+        const int r = rb + lane;
+        if (r >= T.r1) break;
+        TA acc[3] = {0, 0, 0};
+        const TL *p = U + T.off + (int64_t)r * 3 * CW;
+#pragma unroll 2
+        for (int g = 0; g < ng; ++g) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                Vec16<TL> d = ld_stream(p + c * CW);
+                TA tv[CW];
+                smem_vec<TA, CW>(ts + c * T.K + g * CW, tv);
+#pragma unroll
+                for (int k = 0; k < CW; ++k) acc[c] += widen<TA>(d.v[k]) * tv[k];
+            }
+            p += gstride;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) slots[3 * ((int64_t)T.slot + r) + c] = acc[c];
     }
 }
 
 // ------------------------------------------------------------------ kernel 3
-template <typename TL, typename TA>
-__global__ void __launch_bounds__(256)
-k_u(const UItem *__restrict__ items, int64_t n_items, const TL *__restrict__ U, const TA *__restrict__ t,
-    TA *__restrict__ slots)
-{
-    constexpr int CW = 16 / sizeof(TL);
-    const int lane = threadIdx.x & 31;
-    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (w >= n_items) return;
-    const UItem it = items[w];
-    const int r = it.r + lane;
-    if (r >= it.m) return;
-    TA acc[3] = {0, 0, 0};
-    const TL *p = U + it.off + (int64_t)r * 3 * CW;
-    const int64_t gstride = (int64_t)it.m * 3 * CW;
-    const TA *tp = t + it.tp;  // t[c*K + q]
-    const int ng = it.K / CW;
-#pragma unroll 2
-    for (int g = 0; g < ng; ++g) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            Vec16<TL> d = ld_stream(p + c * CW);
-#pragma unroll
-            for (int k = 0; k < CW; ++k) acc[c] += widen<TA>(d.v[k]) * tp[c * it.K + g * CW + k];
-        }
-        p += gstride;
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) slots[3 * ((int64_t)it.slot + r) + c] = acc[c];
-}
-
-// ------------------------------------------------------------------ kernel 4
 // y[3i+c] = sum of row i's slots (in list order) + add[c][i] (FP64), for rows of leaf clusters.
 template <typename TA>
 __global__ void k_rowsum(int n, const int32_t *__restrict__ leaf_of_row, const int32_t *__restrict__ leaf_ptr,
@@ -203,7 +237,26 @@ __global__ void k_rowsum(int n, const int32_t *__restrict__ leaf_of_row, const i
     if (i >= n) return;
     const int l = leaf_of_row[i];
     double a0 = 0, a1 = 0, a2 = 0;
-    for (int k = leaf_ptr[l]; k < leaf_ptr[l + 1]; ++k) {
+    const int k0 = leaf_ptr[l], k1 = leaf_ptr[l + 1];
+    int k = k0;
+    // four slots per iteration: independent loads in flight, summed in list order
+    for (; k + 4 <= k1; k += 4) {
+        TA v[12];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t s = 3 * ((int64_t)leaf_off[k + u] + i);
+            v[3 * u] = slots[s];
+            v[3 * u + 1] = slots[s + 1];
+            v[3 * u + 2] = slots[s + 2];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            a0 += (double)v[3 * u];
+            a1 += (double)v[3 * u + 1];
+            a2 += (double)v[3 * u + 2];
+        }
+    }
+    for (; k < k1; ++k) {
         const int64_t s = 3 * ((int64_t)leaf_off[k] + i);
         a0 += (double)slots[s];
         a1 += (double)slots[s + 1];
@@ -218,7 +271,7 @@ __global__ void k_rowsum(int n, const int32_t *__restrict__ leaf_of_row, const i
 }
 
 // ------------------------------------------------------------------ host entry
-// Packed operator description (device pointers) -- mirrors pq3d_hm_plan in include/pq3d.h.
+// Packed operator description (device pointers) -- mirrors the Python HM_PLAN record.
 struct HmPlan {
     int32_t n;             // elements
     int32_t dtype;         // 0: FP64 dense + FP64 low rank; 1: FP32 + FP32; 2: FP32 dense + BF16 low rank
@@ -227,11 +280,10 @@ struct HmPlan {
     const void *V;         // packed V factors
     const void *ditems;    // DenseItem[n_ditems]
     const void *vitems;    // VItem[n_vitems]
-    const void *uitems;    // UItem[n_uitems]
-    const void *tblocks;   // TBlock[n_lr]
+    const void *utasks;    // UTask[n_utasks]
     const int32_t *leaf_of_row, *leaf_ptr, *leaf_off;
-    int64_t n_ditems, n_vitems, n_uitems, n_lr;
-    int64_t n_slots, n_tpart, n_t;
+    int64_t n_ditems, n_vitems, n_utasks, n_slots, n_tpart;
+    int32_t kmax, pad;     // largest K of a low-rank block (shared memory of k_u)
 };
 
 PQ3D_EXPORT size_t pq3d_item_bytes(int kind)
@@ -239,8 +291,7 @@ PQ3D_EXPORT size_t pq3d_item_bytes(int kind)
     switch (kind) {
     case 0: return sizeof(DenseItem);
     case 1: return sizeof(VItem);
-    case 2: return sizeof(UItem);
-    case 3: return sizeof(TBlock);
+    case 2: return sizeof(UTask);
     case 4: return sizeof(DenseBlock);
     case 5: return sizeof(HmPlan);
     }
@@ -248,7 +299,7 @@ PQ3D_EXPORT size_t pq3d_item_bytes(int kind)
 }
 
 template <typename TD, typename TL, typename TA>
-static int run_matvec(const HmPlan &P, const TA *x, TA *slots, TA *tpart, TA *t, const double *add0,
+static int run_matvec(const HmPlan &P, const TA *x, TA *slots, TA *tpart, const double *add0,
                       const double *add1, const double *add2, double *y, cudaStream_t st)
 {
     const int64_t warps1 = P.n_ditems + P.n_vitems;
@@ -256,41 +307,44 @@ static int run_matvec(const HmPlan &P, const TA *x, TA *slots, TA *tpart, TA *t,
         int64_t blocks = (warps1 * 32 + 255) / 256;
         k_dense_v<TD, TL, TA><<<(unsigned)blocks, 256, 0, st>>>(
             (const DenseItem *)P.ditems, P.n_ditems, (const VItem *)P.vitems, P.n_vitems, (const TD *)P.dense,
-            (const TL *)P.V, x, slots, tpart);
+            (const TL *)P.V, x, x_stride(P.n), slots, tpart);
     }
-    if (P.n_lr > 0) {
-        k_treduce<TA><<<(unsigned)P.n_lr, 128, 0, st>>>((const TBlock *)P.tblocks, P.n_lr, tpart, t);
-        int64_t blocks = (P.n_uitems * 32 + 255) / 256;
-        if (blocks > 0)
-            k_u<TL, TA><<<(unsigned)blocks, 256, 0, st>>>((const UItem *)P.uitems, P.n_uitems, (const TL *)P.U, t,
-                                                          slots);
+    if (P.n_utasks > 0) {
+        const size_t smem = (size_t)3 * P.kmax * sizeof(TA);
+        if (smem > 200 * 1024) return PQ3D_ERR_ARG;
+        if (smem > 48 * 1024)
+            PQ3D_CHECK(cudaFuncSetAttribute(k_u<TL, TA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_u<TL, TA><<<(unsigned)P.n_utasks, 256, smem, st>>>((const UTask *)P.utasks, (const TL *)P.U, tpart, slots);
     }
-    k_rowsum<TA><<<(P.n + 255) / 256, 256, 0, st>>>(P.n, P.leaf_of_row, P.leaf_ptr, P.leaf_off, slots, add0,
-                                                     add1, add2, y);
+    if (y)
+        k_rowsum<TA><<<(P.n + 255) / 256, 256, 0, st>>>(P.n, P.leaf_of_row, P.leaf_ptr, P.leaf_off, slots, add0,
+                                                         add1, add2, y);
     return pq3d_launch_status();
 }
 
-// y (n x 3, FP64, tree order) = K x (+ add_c).  x: interleaved deficit, FP64 for dtype 0 and
-// FP32 otherwise, 2*(n + 16) entries with zero padding.  Scratch: slots (3*n_slots),
-// tpart (n_tpart), t (n_t) in the accumulation type (FP64 for dtype 0, FP32 otherwise).
-PQ3D_EXPORT int pq3d_hmatvec(const void *plan_host, const void *d_x, void *d_slots, void *d_tpart, void *d_t,
+// y (n x 3, FP64, tree order) = K x (+ add_c).  x: deficit in the layout of hm_layout.cuh
+// (4 * x_stride(n) entries: interleaved, strike plane, dip plane), FP64 for dtype 0 and
+// FP32 otherwise.  Scratch: slots (3*n_slots) and
+// tpart (n_tpart) in the accumulation type (FP64 for dtype 0, FP32 otherwise).  With
+// d_y == NULL only the per-row slots are written (the step kernel sums them itself).
+PQ3D_EXPORT int pq3d_hmatvec(const void *plan_host, const void *d_x, void *d_slots, void *d_tpart,
                              const double *d_add0, const double *d_add1, const double *d_add2, double *d_y,
                              cudaStream_t stream)
 {
-    if (!plan_host || !d_x || !d_slots || !d_y) return PQ3D_ERR_ARG;
+    if (!plan_host || !d_x || !d_slots) return PQ3D_ERR_ARG;
     const HmPlan &P = *(const HmPlan *)plan_host;
     if (P.n <= 0) return PQ3D_ERR_ARG;
-    if (P.n_lr > 0 && (!d_tpart || !d_t)) return PQ3D_ERR_ARG;
+    if (P.n_vitems > 0 && !d_tpart) return PQ3D_ERR_ARG;
     switch (P.dtype) {
     case 0:
         return run_matvec<double, double, double>(P, (const double *)d_x, (double *)d_slots, (double *)d_tpart,
-                                                  (double *)d_t, d_add0, d_add1, d_add2, d_y, stream);
+                                                  d_add0, d_add1, d_add2, d_y, stream);
     case 1:
-        return run_matvec<float, float, float>(P, (const float *)d_x, (float *)d_slots, (float *)d_tpart,
-                                               (float *)d_t, d_add0, d_add1, d_add2, d_y, stream);
+        return run_matvec<float, float, float>(P, (const float *)d_x, (float *)d_slots, (float *)d_tpart, d_add0,
+                                               d_add1, d_add2, d_y, stream);
     case 2:
         return run_matvec<float, __nv_bfloat16, float>(P, (const float *)d_x, (float *)d_slots, (float *)d_tpart,
-                                                       (float *)d_t, d_add0, d_add1, d_add2, d_y, stream);
+                                                       d_add0, d_add1, d_add2, d_y, stream);
     }
     return PQ3D_ERR_ARG;
 }

@@ -22,15 +22,17 @@ struct RkArgs {
     double *Tno, *Tt1o, *Tt2o, *psi;                        // state (MPa, MPa, MPa, -)
     double *slip1, *slip2, *slipv1, *slipv2, *slipv, *rake, *Tt, *fric, *slip;
     const double *a, *b, *dc, *f0, *shear_loading, *normal_loading, *vplc, *cr0, *sr0;
-    const double *y;     // elastic load rates (n x 3): A1 x, A2 x, B x  (Pa/s)
+    double *y;           // elastic load rates (n x 3): A1 x, A2 x, B x  (Pa/s)
     double *cand;        // 4n scratch
-    double *blk;         // 4 * gridDim scratch (two attempt parities x two maxima) + 2*gridDim
+    double *blk;         // 10 * gridDim scratch: per-CTA maxima [0,4G), [4G,6G); reduced result at 6G
     void *x;             // next deficit, interleaved (2n + padding), FP32 or FP64
     double *ctrl;        // control block (see pq3d.h)
     double *hist;        // per-step history, 6 doubles per step (may be null)
     const double *hforce; // dt replay: if non-null, step s uses h = hforce[s] and is accepted
-    unsigned *bar;       // barrier counter + generation
-    int n, fix_tn, x_fp32, step_index;
+    unsigned *bar;       // bar[0] arrivals, bar[1] generation, bar[2] end-of-step count (zeroed once)
+    const void *slots;   // when fuse_rowsum: per-row partial sums of the H-matvec
+    const int32_t *leaf_of_row, *leaf_ptr, *leaf_off;
+    int n, fix_tn, x_fp32, step_index, fuse_rowsum, slots_fp32;
     double V0, eta, reltol;
 };
 
@@ -42,66 +44,119 @@ __device__ __forceinline__ double nanmax(double a, double b)
     return a > b ? a : b;
 }
 
-__device__ bool grid_sync(unsigned *bar, double *ctrl)
+// Grid-wide NaN-propagating max of four values.  Every CTA reduces its own
+// values and posts them to blk; the CTA that arrives last at the barrier reduces
+// the posted values with all its threads, publishes the result in res and then
+// releases the others (bounded spin: on timeout ctrl[4] = PQ3D_ERR_TIMEOUT and
+// false is returned).  All CTAs return the same four values.
+// bar[0]: arrival count, bar[1]: generation, bar[2]: end-of-step count.
+template <int NT>
+__device__ bool grid_max4(double *v, double *blk, double *res, unsigned *bar, double *ctrl)
 {
+    __shared__ double wred[NT / 32][4];
+    __shared__ int s_last;
+    __shared__ unsigned s_gen;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] = nanmax(v[q], __shfl_down_sync(0xffffffffu, v[q], o));
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) wred[threadIdx.x >> 5][q] = v[q];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double w[4] = {wred[0][0], wred[0][1], wred[0][2], wred[0][3]};
+        for (int k = 1; k < NT / 32; ++k)
+            for (int q = 0; q < 4; ++q) w[q] = nanmax(w[q], wred[k][q]);
+        for (int q = 0; q < 4; ++q) blk[(int64_t)q * gridDim.x + blockIdx.x] = w[q];
+        s_gen = *(volatile unsigned *)(bar + 1);
+        __threadfence();
+        s_last = atomicAdd(bar, 1u) == gridDim.x - 1;
+    }
     __syncthreads();
     bool ok = true;
-    if (threadIdx.x == 0) {
-        volatile unsigned *vgen = bar + 1;
-        const unsigned gen = *vgen;
+    if (s_last) {
         __threadfence();
-        const unsigned arrived = atomicAdd(bar, 1u);
-        if (arrived == gridDim.x - 1) {
+        double m[4] = {0, 0, 0, 0};
+        for (unsigned k = threadIdx.x; k < gridDim.x; k += NT)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) m[q] = nanmax(m[q], __ldcg(blk + (int64_t)q * gridDim.x + k));
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) m[q] = nanmax(m[q], __shfl_down_sync(0xffffffffu, m[q], o));
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) wred[threadIdx.x >> 5][q] = m[q];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int q = 0; q < 4; ++q) {
+                double w = wred[0][q];
+                for (int k = 1; k < NT / 32; ++k) w = nanmax(w, wred[k][q]);
+                __stcg(res + q, w);
+            }
+            __threadfence();
             atomicExch(bar, 0u);
             __threadfence();
             atomicAdd(bar + 1, 1u);
-        } else {
-            long long it = 0;
-            while (*vgen == gen) {
-                if (++it > (1LL << 24)) {
-                    ctrl[4] = (double)PQ3D_ERR_TIMEOUT;
-                    ok = false;
-                    break;
-                }
-                __nanosleep(64);
+        }
+    } else if (threadIdx.x == 0) {
+        long long it = 0;
+        while (*(volatile unsigned *)(bar + 1) == s_gen) {
+            if (++it > (1LL << 24)) {
+                ctrl[4] = (double)PQ3D_ERR_TIMEOUT;
+                ok = false;
+                break;
             }
+            __nanosleep(64);
         }
         __threadfence();
     }
     __syncthreads();
-    return ok;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = __ldcg(res + q);
+    return __syncthreads_and(ok);
 }
+
+#ifndef PQ3D_RK_THREADS
+#define PQ3D_RK_THREADS 256
+#endif
+constexpr int RK_THREADS = PQ3D_RK_THREADS;   // CTA size of the step kernel
 
 struct Deriv {
     double dpsi, dsig, dt1, dt2;
 };
 
-// derivative (src/QDsim.py:760-813); Tno, Tt in MPa, loads in Pa/s.
-__device__ __forceinline__ Deriv derivative(double Tno, double Tt1o, double Tt2o, double state, double a,
-                                            double b, double dc, double f0, double V0, double slipv,
+// derivative (src/QDsim.py:760-813); Tno, Tt in MPa, loads in Pa/s.  The same
+// expressions, with the quotients shared through per-element (ia = 1/a,
+// ib = 1/b, bdc = b/dc) and per-stage (1/(a Tno)) reciprocals.
+__device__ __forceinline__ Deriv derivative(double Tno, double Tt1o, double Tt2o, double state, double ia,
+                                            double ib, double bdc, double f0, double V0, double slipv,
                                             double AdotV1, double AdotV2, double dsigmadt, double shear,
                                             double eta)
 {
     Tno = Tno * 1e6;
     Tt1o = Tt1o * 1e6;
     Tt2o = Tt2o * 1e6;
-    const double aT = a * Tno;
-    const double sa = -state / a;
-    const double e1p = exp(sa + Tt1o / aT), e1m = exp(sa - Tt1o / aT);
-    const double e2p = exp(sa + Tt2o / aT), e2m = exp(sa - Tt2o / aT);
-    const double dV1dtau = 2 * V0 / aT * 0.5 * (e1p + e1m);
-    const double dV2dtau = 2 * V0 / aT * 0.5 * (e2p + e2m);
-    const double aT2 = a * (Tno * Tno);
-    const double dV1dsigma = -2 * V0 * Tt1o / aT2 * 0.5 * (e1p + e1m);
-    const double dV2dsigma = -2 * V0 * Tt2o / aT2 * 0.5 * (e2p + e2m);
-    const double dV1dstate = -2 * V0 / a * 0.5 * (e1p - e1m);
-    const double dV2dstate = -2 * V0 / a * 0.5 * (e2p - e2m);
-    double arg = (f0 - state) / b;
+    const double iaT = ia / Tno;                  // 1 / (a Tno)
+    const double sa = -state * ia;
+    const double e1p = exp(sa + Tt1o * iaT), e1m = exp(sa - Tt1o * iaT);
+    const double e2p = exp(sa + Tt2o * iaT), e2m = exp(sa - Tt2o * iaT);
+    const double g1 = V0 * iaT * (e1p + e1m);     // 2 V0/(a Tno) * cosh-term
+    const double g2 = V0 * iaT * (e2p + e2m);
+    const double dV1dtau = g1, dV2dtau = g2;
+    const double iTno = 1.0 / Tno;
+    const double dV1dsigma = -g1 * Tt1o * iTno;
+    const double dV2dsigma = -g2 * Tt2o * iTno;
+    const double dV1dstate = -V0 * ia * (e1p - e1m);
+    const double dV2dstate = -V0 * ia * (e2p - e2m);
+    double arg = (f0 - state) * ib;
     arg = arg > 700.0 ? 700.0 : (arg < -700.0 ? -700.0 : arg);
-    const double dstatedt = b / dc * (V0 * exp(arg) - slipv);
+    const double dstatedt = bdc * (V0 * exp(arg) - slipv);
     const double dtau1dt = (-AdotV1 + shear - eta * (dV1dsigma * dsigmadt + dV1dstate * dstatedt)) / (1.0 + eta * dV1dtau);
     const double dtau2dt = (-AdotV2 + shear - eta * (dV2dsigma * dsigmadt + dV2dstate * dstatedt)) / (1.0 + eta * dV2dtau);
-    return Deriv{dstatedt, dsigmadt / 1e6, dtau1dt / 1e6, dtau2dt / 1e6};
+    return Deriv{dstatedt, dsigmadt * 1e-6, dtau1dt * 1e-6, dtau2dt * 1e-6};
 }
 
 // Dormand-Prince 5(4) tableau (src/QDsim.py:1002-1032).
@@ -114,11 +169,57 @@ constexpr double B71 = 35. / 384., B73 = 500. / 1113., B74 = 125. / 192., B75 = 
 constexpr double B81 = 5179. / 57600., B83 = 7571. / 16695., B84 = 393. / 640., B85 = -92097. / 339200.,
                  B86 = 187. / 2100., B87 = 1. / 40.;
 
-__global__ void __launch_bounds__(256) k_rk_step(RkArgs A)
+__global__ void __launch_bounds__(RK_THREADS) k_rk_step(RkArgs A)
 {
     const int n = A.n;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t tid0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (A.fuse_rowsum) {
+        // the H-matvec's row reduction (k_rowsum) done here: y[i] = sum of row i's slots
+        for (int64_t i = tid0; i < n; i += stride) {
+            const int l = A.leaf_of_row[i];
+            double a0 = 0, a1 = 0, a2 = 0;
+            const int k0 = A.leaf_ptr[l], k1 = A.leaf_ptr[l + 1];
+            if (A.slots_fp32) {
+                const float *sl = (const float *)A.slots;
+                int k = k0;
+                for (; k + 4 <= k1; k += 4) {   // four independent loads in flight, list-order sums
+                    float v[12];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int64_t s = 3 * ((int64_t)A.leaf_off[k + u] + i);
+                        v[3 * u] = sl[s]; v[3 * u + 1] = sl[s + 1]; v[3 * u + 2] = sl[s + 2];
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) { a0 += (double)v[3 * u]; a1 += (double)v[3 * u + 1]; a2 += (double)v[3 * u + 2]; }
+                }
+                for (; k < k1; ++k) {
+                    const int64_t s = 3 * ((int64_t)A.leaf_off[k] + i);
+                    a0 += (double)sl[s]; a1 += (double)sl[s + 1]; a2 += (double)sl[s + 2];
+                }
+            } else {
+                const double *sl = (const double *)A.slots;
+                int k = k0;
+                for (; k + 4 <= k1; k += 4) {
+                    double v[12];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int64_t s = 3 * ((int64_t)A.leaf_off[k + u] + i);
+                        v[3 * u] = sl[s]; v[3 * u + 1] = sl[s + 1]; v[3 * u + 2] = sl[s + 2];
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) { a0 += v[3 * u]; a1 += v[3 * u + 1]; a2 += v[3 * u + 2]; }
+                }
+                for (; k < k1; ++k) {
+                    const int64_t s = 3 * ((int64_t)A.leaf_off[k] + i);
+                    a0 += sl[s]; a1 += sl[s + 1]; a2 += sl[s + 2];
+                }
+            }
+            A.y[3 * i] = a0;
+            A.y[3 * i + 1] = a1;
+            A.y[3 * i + 2] = a2;
+        }
+    }
     const bool forced = A.hforce != nullptr;
     double h = forced ? A.hforce[A.step_index] : A.ctrl[0];
     int nrjct = 0, attempt = 0;
@@ -129,11 +230,12 @@ __global__ void __launch_bounds__(256) k_rk_step(RkArgs A)
         double m1 = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0;  // max relative errors, NaN-propagating
         for (int64_t i = tid0; i < n; i += stride) {
             const double a = A.a[i], b = A.b[i], dc = A.dc[i], f0 = A.f0[i], sh = A.shear_loading[i];
+            const double ia = 1.0 / a, ib = 1.0 / b, bdc = b / dc;
             const double sv = A.slipv[i];
             const double L1 = A.y[3 * i], L2 = A.y[3 * i + 1];
             const double dsg = A.fix_tn ? A.normal_loading[i] : A.y[3 * i + 2] + A.normal_loading[i];
             const double Tn = A.Tno[i], T1 = A.Tt1o[i], T2 = A.Tt2o[i], ps = A.psi[i];
-#define DER(tn, t1, t2, p) derivative(tn, t1, t2, p, a, b, dc, f0, A.V0, sv, L1, L2, dsg, sh, A.eta)
+#define DER(tn, t1, t2, p) derivative(tn, t1, t2, p, ia, ib, bdc, f0, A.V0, sv, L1, L2, dsg, sh, A.eta)
             const Deriv k1 = DER(Tn, T1, T2, ps);
             const Deriv k2 = DER(Tn + h * B21 * k1.dsig, T1 + h * B21 * k1.dt1, T2 + h * B21 * k1.dt2, ps + h * B21 * k1.dpsi);
             const Deriv k3 = DER(Tn + h * (B31 * k1.dsig + B32 * k2.dsig), T1 + h * (B31 * k1.dt1 + B32 * k2.dt1),
@@ -171,30 +273,9 @@ __global__ void __launch_bounds__(256) k_rk_step(RkArgs A)
             g2 = nanmax(g2, fabs(fabs(y82 - y52) / y82));
             g3 = nanmax(g3, fabs(fabs(y8n - y5n) / y8n));
         }
-        // block reduction of (m1, g1, g2, g3)
-        double v[4] = {m1, g1, g2, g3};
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v[q] = nanmax(v[q], __shfl_down_sync(0xffffffffu, v[q], o));
-        __shared__ double wred[8][4];
-        if ((threadIdx.x & 31) == 0)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) wred[threadIdx.x >> 5][q] = v[q];
-        __syncthreads();
-        const int par = attempt & 1;
-        if (threadIdx.x == 0) {
-            double w[4] = {wred[0][0], wred[0][1], wred[0][2], wred[0][3]};
-            for (int k = 1; k < (int)(blockDim.x >> 5); ++k)
-                for (int q = 0; q < 4; ++q) w[q] = nanmax(w[q], wred[k][q]);
-            for (int q = 0; q < 4; ++q) A.blk[(int64_t)(par * 4 + q) * gridDim.x + blockIdx.x] = w[q];
-        }
-        if (!grid_sync(A.bar, A.ctrl)) return;
-        // every CTA reduces the per-CTA maxima in the same order -> identical decision
-        double E[4] = {0, 0, 0, 0};
-        for (unsigned k = 0; k < gridDim.x; ++k)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) E[q] = nanmax(E[q], A.blk[(int64_t)(par * 4 + q) * gridDim.x + k]);
+        // grid-wide maxima of (m1, g1, g2, g3); identical in every CTA
+        double E[4] = {m1, g1, g2, g3};
+        if (!grid_max4<RK_THREADS>(E, A.blk, A.blk + 6 * (int64_t)gridDim.x, A.bar, A.ctrl)) return;
         const double R1 = E[0] + 1e-10;
         const double R2 = py_max(py_max(E[1], E[2]), E[3]) + 1e-10;
         const double c1 = R1 / A.reltol, c2 = R2 / A.reltol;
@@ -237,12 +318,20 @@ __global__ void __launch_bounds__(256) k_rk_step(RkArgs A)
             A.fric[i] = A.Tt[i] / Tn;
             const double x1 = v1 - A.vplc[i] * A.cr0[i];
             const double x2 = v2 - A.vplc[i] * A.sr0[i];
+            // interleaved copy (dense blocks) and strike / dip planes (V rows)
+            const int64_t P = ((n + 16 + 7) / 8) * 8;
             if (A.x_fp32) {
-                ((float *)A.x)[2 * i] = (float)x1;
-                ((float *)A.x)[2 * i + 1] = (float)x2;
+                float *xf = (float *)A.x;
+                xf[2 * i] = (float)x1;
+                xf[2 * i + 1] = (float)x2;
+                xf[2 * P + i] = (float)x1;
+                xf[3 * P + i] = (float)x2;
             } else {
-                ((double *)A.x)[2 * i] = x1;
-                ((double *)A.x)[2 * i + 1] = x2;
+                double *xd = (double *)A.x;
+                xd[2 * i] = x1;
+                xd[2 * i + 1] = x2;
+                xd[2 * P + i] = x1;
+                xd[3 * P + i] = x2;
             }
             mv1 = fmax(mv1, fabs(v1));
             mv2 = fmax(mv2, fabs(v2));
@@ -253,22 +342,40 @@ __global__ void __launch_bounds__(256) k_rk_step(RkArgs A)
         mv1 = fmax(mv1, __shfl_down_sync(0xffffffffu, mv1, o));
         mv2 = fmax(mv2, __shfl_down_sync(0xffffffffu, mv2, o));
     }
-    __shared__ double vred[8][2];
+    __shared__ double vred[RK_THREADS / 32][2];
+    __shared__ int s_done;
     if ((threadIdx.x & 31) == 0) { vred[threadIdx.x >> 5][0] = mv1; vred[threadIdx.x >> 5][1] = mv2; }
     __syncthreads();
+    // the last CTA to finish the step reduces the slip-rate maxima and updates ctrl
     if (threadIdx.x == 0) {
         double w1 = vred[0][0], w2 = vred[0][1];
-        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) { w1 = fmax(w1, vred[k][0]); w2 = fmax(w2, vred[k][1]); }
-        A.blk[(int64_t)8 * gridDim.x + blockIdx.x] = w1;
-        A.blk[(int64_t)9 * gridDim.x + blockIdx.x] = w2;
+        for (int k = 1; k < RK_THREADS / 32; ++k) { w1 = fmax(w1, vred[k][0]); w2 = fmax(w2, vred[k][1]); }
+        A.blk[(int64_t)4 * gridDim.x + blockIdx.x] = w1;
+        A.blk[(int64_t)5 * gridDim.x + blockIdx.x] = w2;
+        __threadfence();
+        s_done = atomicAdd(A.bar + 2, 1u) == gridDim.x - 1;
     }
-    if (!grid_sync(A.bar, A.ctrl)) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        double w1 = 0, w2 = 0;
-        for (unsigned k = 0; k < gridDim.x; ++k) {
-            w1 = fmax(w1, A.blk[(int64_t)8 * gridDim.x + k]);
-            w2 = fmax(w2, A.blk[(int64_t)9 * gridDim.x + k]);
-        }
+    __syncthreads();
+    if (!s_done) return;
+    __threadfence();
+    double w1 = 0, w2 = 0;
+    for (unsigned k = threadIdx.x; k < gridDim.x; k += RK_THREADS) {
+        w1 = fmax(w1, __ldcg(A.blk + (int64_t)4 * gridDim.x + k));
+        w2 = fmax(w2, __ldcg(A.blk + (int64_t)5 * gridDim.x + k));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        w1 = fmax(w1, __shfl_down_sync(0xffffffffu, w1, o));
+        w2 = fmax(w2, __shfl_down_sync(0xffffffffu, w2, o));
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) { vred[threadIdx.x >> 5][0] = w1; vred[threadIdx.x >> 5][1] = w2; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        w1 = vred[0][0];
+        w2 = vred[0][1];
+        for (int k = 1; k < RK_THREADS / 32; ++k) { w1 = fmax(w1, vred[k][0]); w2 = fmax(w2, vred[k][1]); }
+        A.bar[2] = 0u;
         if (accepted) {
             const double t = A.ctrl[2] + h;
             A.ctrl[2] = t;
@@ -302,8 +409,8 @@ PQ3D_EXPORT int pq3d_rk_grid(int n)
     int dev = 0, sms = 0, per = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rk_step, 256, 0) != cudaSuccess) return -1;
-    int need = (n + 255) / 256;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rk_step, RK_THREADS, 0) != cudaSuccess) return -1;
+    int need = (n + RK_THREADS - 1) / RK_THREADS;
     int cap = sms * per;
     return need < cap ? need : cap;
 }
@@ -317,7 +424,7 @@ PQ3D_EXPORT int pq3d_rk_step(const void *args, int grid, cudaStream_t stream)
     if (A.n <= 0 || !A.ctrl || !A.bar || !A.blk || !A.cand || !A.y || !A.x) return PQ3D_ERR_ARG;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid);
-    cfg.blockDim = dim3(256);
+    cfg.blockDim = dim3(RK_THREADS);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
@@ -344,7 +451,7 @@ PQ3D_EXPORT int pq3d_rk_step(const void *args, int grid, cudaStream_t stream)
 // counter is cleared on the stream before each launch, and calls that overlap
 // on the GPU (different streams, or several threads) race on it.
 #define PQ3D_NOALLOC_MAX_N 131072
-#define PQ3D_NOALLOC_MAX_GRID 4096
+#define PQ3D_NOALLOC_MAX_GRID 4096   // CTAs of RK_THREADS threads
 
 static __device__ __align__(256) double g_rk_scratch[4 * PQ3D_NOALLOC_MAX_N + 10 * PQ3D_NOALLOC_MAX_GRID + 2];
 
@@ -393,11 +500,11 @@ PQ3D_EXPORT int pq3d_rk_step_noalloc(const void *args, int grid, cudaStream_t st
     A.cand = s;
     A.blk = s + 4 * (size_t)PQ3D_NOALLOC_MAX_N;
     A.bar = (unsigned *)(s + 4 * (size_t)PQ3D_NOALLOC_MAX_N + 10 * (size_t)PQ3D_NOALLOC_MAX_GRID);
-    // the barrier counter must start at zero; the rest is written before it is read
-    PQ3D_CHECK(cudaMemsetAsync(A.bar, 0, 2 * sizeof(unsigned), stream));
+    // the barrier counters must start at zero; the rest is written before it is read
+    PQ3D_CHECK(cudaMemsetAsync(A.bar, 0, 4 * sizeof(unsigned), stream));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid);
-    cfg.blockDim = dim3(256);
+    cfg.blockDim = dim3(RK_THREADS);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];

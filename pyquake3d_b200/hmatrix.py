@@ -194,19 +194,37 @@ def aca_start_indices(blocks, seed):
 # ----------------------------------------------------------------------------- packed layout (host)
 
 
+def x_stride(n):
+    """Plane stride of the device deficit vector (hm_layout.cuh x_stride)."""
+    return ((n + 16 + 7) // 8) * 8
+
+
+def pack_x(x1, x2, n):
+    """Deficit vector in the device layout: interleaved pairs, then strike and dip
+    planes (x1, x2 already in tree order)."""
+    P = x_stride(n)
+    x = np.zeros(4 * P)
+    x[0:2 * n:2] = x1
+    x[1:2 * n:2] = x2
+    x[2 * P:2 * P + n] = x1
+    x[3 * P:3 * P + n] = x2
+    return x
+
+
 def dense_layout(dense_blocks):
-    """DenseBlock records with FP64 / FP32 offsets, and the two array sizes."""
+    """DenseBlock records with FP64 / FP32 offsets, and the two array sizes.  Stored
+    columns start at the column-group-aligned c0 - (c0 % CW)."""
     recs = np.zeros(len(dense_blocks), dtype=_lib.DENSE_BLOCK)
     off64 = off32 = 0
     for i, b in enumerate(dense_blocks):
-        m, n = len(b.row.indices), len(b.col.indices)
-        recs[i] = (off64, off32, m, n, b.row.start, b.col.start)
-        off64 += _cdiv(n, 2) * m * 12
-        off32 += _cdiv(n, 4) * m * 24
+        m, n, c0 = len(b.row.indices), len(b.col.indices), b.col.start
+        recs[i] = (off64, off32, m, n, b.row.start, c0)
+        off64 += _cdiv(n + c0 % 2, 2) * m * 12
+        off32 += _cdiv(n + c0 % 4, 4) * m * 24
     return recs, off64, off32
 
 
-def build_plan_arrays(struct, dense_recs, kS, kD, code, dense_chunk=64, v_chunk=64):
+def build_plan_arrays(struct, dense_recs, kS, kD, code, dense_chunk=64, v_chunk=256, u_rows=512):
     """Matvec work items, slot layout and per-leaf slot lists for storage code
     (0 FP64, 1 FP32, 2 FP32 dense + BF16 low rank).  Pure numpy.
 
@@ -221,17 +239,19 @@ def build_plan_arrays(struct, dense_recs, kS, kD, code, dense_chunk=64, v_chunk=
     dense_off = dense_recs["off64"] if code == 0 else dense_recs["off32"]
     for i in range(len(dense_recs)):
         m, nn, r0, c0 = (int(dense_recs[k][i]) for k in ("m", "n", "r0", "c0"))
-        ng = _cdiv(nn, cwd)
+        lead = c0 % cwd
+        ng = _cdiv(nn + lead, cwd)
         for g0 in range(0, ng, dense_chunk):
             g1 = min(ng, g0 + dense_chunk)
             for r in range(0, m, 32):
-                ditems.append((int(dense_off[i]), m, r, g0, g1, c0, slot))
+                ditems.append((int(dense_off[i]), m, r, g0, g1, c0 - lead, slot))
             slot_rows.append((slot, r0, m))
             slot += m
     aca_blocks = [b for b in struct.blocks if b.aca]
-    u_off = v_off = tp = tb = 0
-    vitems, uitems, tblocks, pack = [], [], [], []
+    u_off = v_off = tp = 0
+    vitems, utasks, pack = [], [], []
     lr_entries = 0
+    kmax = 0
     for bi, b in enumerate(aca_blocks):
         m, nn = len(b.row.indices), len(b.col.indices)
         ks, kd = int(kS[bi]), int(kD[bi])
@@ -239,25 +259,27 @@ def build_plan_arrays(struct, dense_recs, kS, kD, code, dense_chunk=64, v_chunk=
         if ks + kd == 0:
             continue
         K = _cdiv(ks + kd, cwl) * cwl
+        kmax = max(kmax, K)
         Q = 3 * (ks + kd)
-        ngv = _cdiv(nn, cwl)
+        lead = b.col.start % cwl
+        ngv = _cdiv(nn + lead, cwl)
+        npad = ngv * cwl
         nch = _cdiv(ngv, v_chunk)
         for ch in range(nch):
             g0 = ch * v_chunk
             g1 = min(ngv, g0 + v_chunk)
-            for q in range(0, Q, 32):
-                vitems.append((v_off, Q, q, g0, g1, b.col.start, ks, tp + ch * Q))
-        tblocks.append((ks, kd, K, Q, tp, nch, tb, 0))
-        for r in range(0, m, 32):
-            uitems.append((u_off, m, r, K, ks, kd, slot, tb, nch))
+            for s_, (qa, qb) in enumerate(((0, 3 * ks), (3 * ks, Q))):
+                for q in range(qa, qb, 8):
+                    vitems.append((v_off, Q, q, min(8, qb - q), g0, g1, b.col.start - lead, s_, tp + ch * Q))
+        for r0 in range(0, m, u_rows):
+            utasks.append((u_off, m, r0, min(m, r0 + u_rows), K, ks, kd, Q, tp, nch, slot))
         slot_rows.append((slot, b.row.start, m))
         for p in (0, 1):
             pack.append((bi, p, u_off, v_off, K, Q, ks, kd))
         slot += m
         tp += nch * Q
-        tb += 3 * K
         u_off += (K // cwl) * m * 3 * cwl
-        v_off += ngv * Q * cwl
+        v_off += Q * npad
     nleaf = len(struct.leaves)
     leaf_of_row = np.empty(n, dtype=np.int32)
     for lf in struct.leaves:
@@ -280,9 +302,8 @@ def build_plan_arrays(struct, dense_recs, kS, kD, code, dense_chunk=64, v_chunk=
     esz_d = 8 if code == 0 else 4
     esz_l = {0: 8, 1: 4, 2: 2}[code]
     dense_entries = int(np.sum(dense_recs["m"].astype(np.int64) * dense_recs["n"])) if len(dense_recs) else 0
-    return dict(ditems=rec(ditems, _lib.DENSE_ITEM), vitems=rec(vitems, _lib.V_ITEM), uitems=rec(uitems, _lib.U_ITEM),
-                tblocks=rec(tblocks, _lib.T_BLOCK), n_ditems=len(ditems), n_vitems=len(vitems),
-                n_uitems=len(uitems), n_lr=len(tblocks), n_slots=slot, n_tpart=tp, n_t=tb,
+    return dict(ditems=rec(ditems, _lib.DENSE_ITEM), vitems=rec(vitems, _lib.V_ITEM), utasks=rec(utasks, _lib.U_TASK),
+                n_ditems=len(ditems), n_vitems=len(vitems), n_utasks=len(utasks), n_slots=slot, n_tpart=tp, kmax=kmax,
                 u_size=u_off, v_size=v_off, pack=pack, leaf_of_row=leaf_of_row, leaf_ptr=leaf_ptr,
                 leaf_off=leaf_off if len(leaf_off) else np.zeros(1, np.int32), slot_rows=sr,
                 alg_bytes=dense_entries * 6 * esz_d + lr_entries * esz_l + 2 * n * esz_d + 3 * n * 8)
@@ -311,7 +332,7 @@ class DeviceHMatrix:
     V_CHUNK_GROUPS = 64       # column groups per V work item
 
     def __init__(self, struct, xg, ev, nodes, tri, mu, lam, device="cuda", aca_tol=0.01, aca_rel=False,
-                 aca_seed=0, kcap=96, ws_budget_bytes=8 << 30):
+                 aca_seed=0, kcap=96, ws_budget_bytes=8 << 30, keep_factors=False):
         import torch
         self.torch = torch
         self.L = _lib.load()
@@ -321,6 +342,7 @@ class DeviceHMatrix:
         self.dev = torch.device(device)
         self.aca_tol, self.aca_rel, self.aca_seed = float(aca_tol), bool(aca_rel), int(aca_seed)
         self.kcap = int(kcap)
+        self.keep_factors = bool(keep_factors)
         self.ws_budget = int(ws_budget_bytes)
         f64 = dict(dtype=torch.float64, device=self.dev)
         self.xg = torch.tensor(np.ascontiguousarray(xg), **f64)
@@ -360,6 +382,10 @@ class DeviceHMatrix:
         torch.cuda.synchronize()
         self.timings["pack_s"] = time.perf_counter() - t2
         self.assembled = True
+        if not self.keep_factors:
+            # packed copies are all that the matvec needs: release the FP64 ACA workspaces
+            self.aca_ws = [(None, keep) for _, keep in self.aca_ws]
+            torch.cuda.empty_cache()
         return self
 
     def _assemble_dense(self, want):
@@ -466,6 +492,9 @@ class DeviceHMatrix:
     def plan(self, dtype):
         if dtype in self.plans:
             return self.plans[dtype]
+        if self.assembled and not self.keep_factors and self.aca_blocks:
+            raise _lib.Pq3dError("ACA factors were released after assembly; request every precision in "
+                                 "assemble(want=...) or construct with keep_factors=True")
         torch = self.torch
         code = DTYPES[dtype]
         kS, kD = self.ranks()
@@ -496,22 +525,20 @@ class DeviceHMatrix:
         acc = torch.float64 if code == 0 else torch.float32
         P = dict(code=code, dtype=dtype, acc=acc,
                  dense=self.dense64 if code == 0 else self.dense32, U=Ubuf, V=Vbuf,
-                 ditems=dev_rec(A["ditems"]), vitems=dev_rec(A["vitems"]), uitems=dev_rec(A["uitems"]),
-                 tblocks=dev_rec(A["tblocks"]),
+                 ditems=dev_rec(A["ditems"]), vitems=dev_rec(A["vitems"]), utasks=dev_rec(A["utasks"]),
                  leaf_of_row=torch.tensor(A["leaf_of_row"], device=self.dev),
                  leaf_ptr=torch.tensor(A["leaf_ptr"], device=self.dev),
                  leaf_off=torch.tensor(A["leaf_off"], device=self.dev),
-                 n_ditems=A["n_ditems"], n_vitems=A["n_vitems"], n_uitems=A["n_uitems"], n_lr=A["n_lr"],
-                 n_slots=A["n_slots"], n_tpart=A["n_tpart"], n_t=A["n_t"])
+                 n_ditems=A["n_ditems"], n_vitems=A["n_vitems"], n_utasks=A["n_utasks"],
+                 n_slots=A["n_slots"], n_tpart=A["n_tpart"], kmax=A["kmax"])
         P["slots"] = torch.empty(3 * max(P["n_slots"], 1), dtype=acc, device=self.dev)
         P["tpart"] = torch.empty(max(P["n_tpart"], 1), dtype=acc, device=self.dev)
-        P["t"] = torch.empty(max(P["n_t"], 1), dtype=acc, device=self.dev)
         hp = np.zeros(1, dtype=_lib.HM_PLAN)
         hp["n"] = self.n
         hp["dtype"] = code
-        for k in ("dense", "U", "V", "ditems", "vitems", "uitems", "tblocks", "leaf_of_row", "leaf_ptr", "leaf_off"):
+        for k in ("dense", "U", "V", "ditems", "vitems", "utasks", "leaf_of_row", "leaf_ptr", "leaf_off"):
             hp[k] = P[k].data_ptr() if P[k] is not None else 0
-        for k in ("n_ditems", "n_vitems", "n_uitems", "n_lr", "n_slots", "n_tpart", "n_t"):
+        for k in ("n_ditems", "n_vitems", "n_utasks", "n_slots", "n_tpart", "kmax"):
             hp[k] = P[k]
         P["host_plan"] = hp
         P["alg_bytes"] = A["alg_bytes"]
@@ -532,27 +559,27 @@ class DeviceHMatrix:
         return self._ro_cache
 
     def new_x(self, dtype):
-        """Zero interleaved deficit buffer (tree order) with padding for the given plan."""
+        """Zero deficit buffer (tree order, device layout of pack_x) for the given plan."""
         P = self.plan(dtype)
-        return self.torch.zeros(2 * (self.n + 16), dtype=P["acc"], device=self.dev)
+        return self.torch.zeros(4 * x_stride(self.n), dtype=P["acc"], device=self.dev)
 
-    def matvec(self, x, dtype, y=None, add=(None, None, None), stream=None):
-        """y[i, c] = sum_j K_c(i, j) x  (tree order, FP64 output)."""
+    def matvec(self, x, dtype, y=None, add=(None, None, None), stream=None, slots_only=False):
+        """y[i, c] = sum_j K_c(i, j) x  (tree order, FP64 output).  slots_only: write the
+        per-row partial sums only (the step kernel reduces them)."""
         P = self.plan(dtype)
-        if y is None:
+        if y is None and not slots_only:
             y = self.torch.empty((self.n, 3), dtype=self.torch.float64, device=self.dev)
         st = _lib.stream_ptr(stream)
-        check(self.L.pq3d_hmatvec(P["host_plan"].ctypes.data, ptr(x), ptr(P["slots"]), ptr(P["tpart"]), ptr(P["t"]),
-                                  ptr(add[0]), ptr(add[1]), ptr(add[2]), ptr(y), st), "pq3d_hmatvec")
+        check(self.L.pq3d_hmatvec(P["host_plan"].ctypes.data, ptr(x), ptr(P["slots"]), ptr(P["tpart"]),
+                                  ptr(add[0]), ptr(add[1]), ptr(add[2]), None if slots_only else ptr(y), st),
+              "pq3d_hmatvec")
         return y
 
     def apply(self, x1, x2, dtype="fp64"):
         """Host convenience: (y1, y2, yB) in element order for deficits x1, x2 (element order)."""
         torch = self.torch
         P = self.plan(dtype)
-        xt = np.zeros(2 * (self.n + 16))
-        xt[0:2 * self.n:2] = np.asarray(x1)[self.s.perm]
-        xt[1:2 * self.n:2] = np.asarray(x2)[self.s.perm]
+        xt = pack_x(np.asarray(x1)[self.s.perm], np.asarray(x2)[self.s.perm], self.n)
         x = torch.tensor(xt, dtype=P["acc"], device=self.dev)
         y = self.matvec(x, dtype).cpu().numpy()
         out = np.empty_like(y)
@@ -574,10 +601,11 @@ def export_blocks(op):
     recs = op.dense_recs
     for i in range(len(recs)):
         m, n, r0, c0 = (int(recs[k][i]) for k in ("m", "n", "r0", "c0"))
-        ng = _cdiv(n, 2)
+        lead = c0 % 2
+        ng = _cdiv(n + lead, 2)
         a = dense[int(recs["off64"][i]):int(recs["off64"][i]) + ng * m * 12].reshape(ng, m, 3, 2, 2)
         # (group, row, comp, slip, t) -> (slip, comp, row, col)
-        M = a.transpose(3, 2, 1, 0, 4).reshape(2, 3, m, ng * 2)[:, :, :, :n].reshape(6, m, n)
+        M = a.transpose(3, 2, 1, 0, 4).reshape(2, 3, m, ng * 2)[:, :, :, lead:lead + n].reshape(6, m, n)
         out.append(("dense", perm[r0:r0 + m], perm[c0:c0 + n], np.ascontiguousarray(M)))
     kS, kD = op.ranks()
     u_off = v_off = 0
@@ -592,9 +620,10 @@ def export_blocks(op):
             continue
         K = _cdiv(ks + kd, 2) * 2
         Q = 3 * (ks + kd)
-        ngv = _cdiv(n, 2)
+        lead = b.col.start % 2
+        ngv = _cdiv(n + lead, 2)
         Ub = U[u_off:u_off + K // 2 * m * 6].reshape(K // 2, m, 3, 2).transpose(2, 1, 0, 3).reshape(3, m, K)
-        Vb = V[v_off:v_off + ngv * Q * 2].reshape(ngv, Q, 2).transpose(1, 0, 2).reshape(Q, ngv * 2)[:, :n]
+        Vb = V[v_off:v_off + ngv * Q * 2].reshape(ngv, Q, 2).transpose(1, 0, 2).reshape(Q, ngv * 2)[:, lead:lead + n]
         S, D = {}, {}
         for c, (un, vn) in enumerate((("U1", "V1"), ("U2", "V2"), ("UB", "VB"))):
             S[un] = np.ascontiguousarray(Ub[c, :, :ks])

@@ -324,7 +324,7 @@ class BlockTree:
         tol = float(P.get("ACA tolerance", 0.01))
         rel = P.get("ACA relative tolerance", "False") == "True"
         seed = int(P.get("ACA seed", 0))
-        want = ("fp64",) if sim.precision == "fp64" else ("fp64", sim.precision)
+        want = getattr(self, "want", None) or (("fp64",) if sim.precision == "fp64" else ("fp64", sim.precision))
         self._op = DeviceHMatrix(self.struct, sim.xg, sim.eleVec, sim.nodelst, sim.elelst, sim.mu, sim.lambda_,
                                  device=sim.device, aca_tol=tol, aca_rel=rel, aca_seed=seed).assemble(want)
         return self._op
@@ -378,15 +378,15 @@ class DeviceStepper:
             raise _lib.Pq3dError("pq3d_rk_grid failed")
         self.blk = torch.zeros(10 * self.grid, **f64)
         self.ctrl = torch.zeros(16, **f64)
-        self.bar = torch.zeros(2, dtype=torch.int32, device=dev)
+        self.bar = torch.zeros(4, dtype=torch.int32, device=dev)
         self.hist = None
         self.hist_cap = 0
         self.hforce = None
         self.hforce_cap = 0
         self.x = op.new_x(precision)
-        x0 = np.zeros(2 * (n + 16))
-        x0[0:2 * n:2] = (sim.slipv1 - sim.slipvC * np.cos(sim.rake0))[self.perm]
-        x0[1:2 * n:2] = (sim.slipv2 - sim.slipvC * np.sin(sim.rake0))[self.perm]
+        from .hmatrix import pack_x
+        x0 = pack_x((sim.slipv1 - sim.slipvC * np.cos(sim.rake0))[self.perm],
+                    (sim.slipv2 - sim.slipvC * np.sin(sim.rake0))[self.perm], n)
         self.x.copy_(torch.tensor(x0, dtype=self.x.dtype))
         self.V0 = sim.V0
         self.eta = sim.mu / (2.0 * sim.Cs)
@@ -407,13 +407,21 @@ class DeviceStepper:
         self.args["n"] = n
         self.args["fix_tn"] = self.fix_tn
         self.args["x_fp32"] = 0 if self.x.dtype == torch.float64 else 1
+        P = op.plan(precision)
+        self.args["slots"] = P["slots"].data_ptr()
+        self.args["leaf_of_row"] = P["leaf_of_row"].data_ptr()
+        self.args["leaf_ptr"] = P["leaf_ptr"].data_ptr()
+        self.args["leaf_off"] = P["leaf_off"].data_ptr()
+        self.args["fuse_rowsum"] = 1
+        self.args["slots_fp32"] = 0 if P["acc"] == torch.float64 else 1
         self.args["V0"] = self.V0
         self.args["eta"] = self.eta
         self.args["reltol"] = self.reltol
 
     def launch(self, step_index=0, stream=None):
-        """Enqueue one step (matvec + DP5(4) kernel) without host synchronization."""
-        self.op.matvec(self.x, self.precision, y=self.y, stream=stream)
+        """Enqueue one step (matvec + DP5(4) kernel) without host synchronization; the
+        step kernel reduces the matvec's per-row slots itself."""
+        self.op.matvec(self.x, self.precision, stream=stream, slots_only=True)
         self.args["step_index"] = step_index
         # per-step records only while the buffers have room for this step index
         self.args["hist"] = self.hist.data_ptr() if self.hist is not None and step_index < self.hist_cap else 0
@@ -440,6 +448,27 @@ class DeviceStepper:
         self.steps += 1
         self.time = float(c[2])
         return float(c[1]), float(c[0])
+
+    def capture(self, nsteps):
+        """CUDA graph of nsteps consecutive steps (matvec + step kernel each).  The
+        step size is carried on the device (ctrl[0]), so replays chain; step s of a
+        replay writes history row s.  Returns None if capture is not possible here."""
+        torch = self.torch
+        if self.hist is None or self.hist_cap < nsteps:
+            self.set_history(nsteps)
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        try:
+            with torch.cuda.stream(s):
+                with torch.cuda.graph(g, stream=s):
+                    for i in range(nsteps):
+                        self.launch(i)
+        except (RuntimeError, _lib.Pq3dError):
+            torch.cuda.synchronize()
+            return None
+        torch.cuda.current_stream().wait_stream(s)
+        return g
 
     def run(self, nsteps, dttry):
         """nsteps steps back to back on the device; returns the history (nsteps x 6)."""

@@ -5,13 +5,13 @@ packed into the device layouts with the same index formulas the CUDA kernels
 use (hm_layout.cuh: dense_index, u_index, v_index; k_dense_assemble and
 k_aca_pack write that way), then the work items, slots and per-leaf slot lists
 from build_plan_arrays are executed by numpy emulations of k_dense_v,
-k_treduce, k_u and k_rowsum.  The result must equal the oracle's
+k_u and k_rowsum.  The result must equal the oracle's
 blocks_process_MVM products."""
 import numpy as np
 import pytest
 
 import qd_oracle
-from pyquake3d_b200.hmatrix import aca_start_indices, build_plan_arrays, dense_layout
+from pyquake3d_b200.hmatrix import aca_start_indices, build_plan_arrays, dense_layout, pack_x, x_stride
 
 CW_D = {0: 2, 1: 4, 2: 4}
 CW_L = {0: 2, 1: 4, 2: 8}
@@ -25,8 +25,8 @@ def u_index(m, i, c, q, cw):
     return ((q // cw) * m + i) * (3 * cw) + c * cw + (q % cw)
 
 
-def v_index(Q, q, j, cw):
-    return ((j // cw) * Q + q) * cw + (j % cw)
+def v_index(Q, q, jj, cw):
+    return ((jj // cw) * Q + q) * cw + (jj % cw)
 
 
 @pytest.fixture(scope="module")
@@ -53,12 +53,12 @@ def pack(st, op, code):
         # tree-local index of each of the block's elements
         ti = st.iperm[b.row.indices] - b.row.start
         tj = st.iperm[b.col.indices] - b.col.start
-        I, J = np.meshgrid(ti, tj, indexing="ij")
+        I, J = np.meshgrid(ti, tj + b.col.start % cwd, indexing="ij")
         for slip in range(2):
             for c in range(3):
                 D[offs[k] + dense_index(m, I, J, c, slip, cwd)] = M[3 * slip + c]
     ranks = np.array(op.ranks()).reshape(-1, 2)
-    A = build_plan_arrays(st, recs, ranks[:, 0], ranks[:, 1], code)
+    A = build_plan_arrays(st, recs, ranks[:, 0], ranks[:, 1], code, dense_chunk=2, v_chunk=3, u_rows=40)
     U = np.zeros(max(A["u_size"], 8))
     V = np.zeros(max(A["v_size"], 8))
     ab = [b for b in st.blocks if b.aca]
@@ -77,12 +77,16 @@ def pack(st, op, code):
             for q in range(k):
                 U[u_off + u_index(m, ti, c, qoff + q, cwl)] = Uc[:, q]
                 row = c * ks + q if p == 0 else 3 * ks + c * kd + q
-                V[v_off + v_index(Q, row, tj, cwl)] = Vc[q]
+                V[v_off + v_index(Q, row, b.col.start % cwl + tj, cwl)] = Vc[q]
     return A, D, U, V
 
 
 def emulate(st, A, D, U, V, x, code):
     cwd, cwl = CW_D[code], CW_L[code]
+    for it in A["ditems"][:A["n_ditems"]]:
+        assert int(it["c0"]) % cwd == 0          # aligned x slices (vector loads)
+    for it in A["vitems"][:A["n_vitems"]]:
+        assert int(it["c0"]) % cwl == 0
     slots = np.zeros(3 * max(A["n_slots"], 1))
     tpart = np.zeros(max(A["n_tpart"], 1))
     for it in A["ditems"][:A["n_ditems"]]:
@@ -98,31 +102,28 @@ def emulate(st, A, D, U, V, x, code):
                             x[2 * (int(it["c0"]) + j) + s]
         slots[3 * (int(it["slot"]) + rr)[:, None] + np.arange(3)] = acc
     for it in A["vitems"][:A["n_vitems"]]:
-        Q, q0 = int(it["Q"]), int(it["q"])
-        qq = np.arange(q0, min(q0 + 32, Q))
-        s = np.where(qq < 3 * int(it["kS"]), 0, 1)
-        acc = np.zeros(len(qq))
-        for g in range(int(it["g0"]), int(it["g1"])):
-            for t in range(cwl):
-                acc += V[it["off"] + (g * Q + qq) * cwl + t] * x[2 * (int(it["c0"]) + g * cwl + t) + s]
-        tpart[int(it["tp"]) + qq] = acc
-    t = np.zeros(max(A["n_t"], 1))
-    for B in A["tblocks"][:A["n_lr"]]:
-        ks, kd, K, Q = int(B["kS"]), int(B["kD"]), int(B["K"]), int(B["Q"])
+        Q, q0, nr, s = int(it["Q"]), int(it["q"]), int(it["nr"]), int(it["s"])
+        for q in range(q0, q0 + nr):
+            acc = 0.0
+            for g in range(int(it["g0"]), int(it["g1"])):
+                for t in range(cwl):
+                    acc += V[it["off"] + (g * Q + q) * cwl + t] * x[(2 + s) * x_stride(st.n) + int(it["c0"]) + g * cwl + t]
+            tpart[int(it["tp"]) + q] = acc
+    for T in A["utasks"][:A["n_utasks"]]:
+        ks, kd, K, Q, m = int(T["kS"]), int(T["kD"]), int(T["K"]), int(T["Q"]), int(T["m"])
+        tv = np.zeros(3 * K)
         for c in range(3):
             for q in range(K):
                 row = c * ks + q if q < ks else (3 * ks + c * kd + q - ks if q < ks + kd else -1)
                 if row >= 0:
-                    t[int(B["tb"]) + c * K + q] = sum(tpart[int(B["tp"]) + ch * Q + row] for ch in range(int(B["nch"])))
-    for it in A["uitems"][:A["n_uitems"]]:
-        m, r0, K = int(it["m"]), int(it["r"]), int(it["K"])
-        rr = np.arange(r0, min(r0 + 32, m))
+                    tv[c * K + q] = sum(tpart[int(T["tp"]) + ch * Q + row] for ch in range(int(T["nch"])))
+        rr = np.arange(int(T["r0"]), int(T["r1"]))
         acc = np.zeros((len(rr), 3))
         for g in range(K // cwl):
             for c in range(3):
                 for k in range(cwl):
-                    acc[:, c] += U[it["off"] + (g * m + rr) * 3 * cwl + c * cwl + k] * t[int(it["tp"]) + c * K + g * cwl + k]
-        slots[3 * (int(it["slot"]) + rr)[:, None] + np.arange(3)] = acc
+                    acc[:, c] += U[T["off"] + (g * m + rr) * 3 * cwl + c * cwl + k] * tv[c * K + g * cwl + k]
+        slots[3 * (int(T["slot"]) + rr)[:, None] + np.arange(3)] = acc
     y = np.zeros((st.n, 3))
     for i in range(st.n):
         lf = A["leaf_of_row"][i]
@@ -137,9 +138,7 @@ def test_packed_matvec_emulation_equals_oracle(setup, code):
     A, D, U, V = pack(st, op, code)
     rng = np.random.default_rng(11)
     x1, x2 = rng.standard_normal((2, st.n))
-    x = np.zeros(2 * (st.n + 16))
-    x[0:2 * st.n:2] = x1[st.perm]
-    x[1:2 * st.n:2] = x2[st.perm]
+    x = pack_x(x1[st.perm], x2[st.perm], st.n)
     y = emulate(st, A, D, U, V, x, code)
     out = np.empty_like(y)
     out[st.perm] = y
@@ -153,7 +152,7 @@ def test_slot_lists_cover_every_row_owner_once(setup):
     st, op = setup
     ranks = np.array(op.ranks()).reshape(-1, 2)
     recs, _, _ = dense_layout([b for b in st.blocks if not b.aca])
-    A = build_plan_arrays(st, recs, ranks[:, 0], ranks[:, 1], 2, dense_chunk=4, v_chunk=2)
+    A = build_plan_arrays(st, recs, ranks[:, 0], ranks[:, 1], 2, dense_chunk=4, v_chunk=2, u_rows=16)
     owner_of_slot = np.full(A["n_slots"], -1)
     for k, (s0, r0, m) in enumerate(A["slot_rows"]):
         owner_of_slot[s0:s0 + m] = k
