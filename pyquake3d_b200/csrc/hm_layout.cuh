@@ -9,15 +9,16 @@
 // is one aligned vector load.
 //
 // Dense block (m x n, six operators): element (row i, col j, comp c, slip s)
-//   at  ((jj / CW) * m + i) * 6*CW + (2*c + s) * CW + (jj % CW),  jj = j + lead
+//   at  (((jj / CW) * 6 + 2*c + s) * m + i) * CW + (jj % CW),  jj = j + lead
 // with comp c in {tau1, tau2, sigma_n} and slip s in {strike, dip}; CW is 4
-// for FP32 and 2 for FP64, so one row's CW columns for all six operators are
-// 96 contiguous bytes and 32 consecutive rows are 3 KB contiguous.
+// for FP32 and 2 for FP64.  For one column group and one operator the rows are
+// consecutive 16-byte pieces, so a warp (lanes over rows) loads 512 contiguous
+// bytes per instruction.
 //
 // Low-rank block (ACA): for comp c the block is U_c T_c with
 //   U_c = [U_cs | U_cd]  (m x K, K = kS + kD, padded to a multiple of CWU)
 //   t_c = [V_cs x_strike ; V_cd x_dip]
-// U element (row i, comp c, q) at ((q / CWU) * m + i) * 3*CWU + c*CWU + q % CWU.
+// U element (row i, comp c, q) at (((q / CWU) * 3 + c) * m + i) * CWU + q % CWU.
 // V rows: Q = 3*kS + 3*kD rows (A1s, A2s, Bs rows first, then A1d, A2d, Bd),
 // column-group major: element (q, j) at ((jj / CWV) * Q + q) * CWV + jj % CWV
 // with jj = lead + j, so 8 consecutive rows of one column group are 128
@@ -42,12 +43,12 @@ struct DenseBlock {
 
 __host__ __device__ inline int64_t dense_index(int m, int i, int j, int comp, int slip, int cw)
 {
-    return ((int64_t)(j / cw) * m + i) * (6 * cw) + (2 * comp + slip) * cw + (j % cw);
+    return (((int64_t)(j / cw) * 6 + 2 * comp + slip) * m + i) * cw + (j % cw);
 }
 
 __host__ __device__ inline int64_t u_index(int m, int i, int comp, int q, int cwu)
 {
-    return ((int64_t)(q / cwu) * m + i) * (3 * cwu) + comp * cwu + (q % cwu);
+    return (((int64_t)(q / cwu) * 3 + comp) * m + i) * cwu + (q % cwu);
 }
 
 __host__ __device__ inline int64_t v_index(int Q, int q, int jj, int cwv)
@@ -62,7 +63,7 @@ struct DenseItem {          // rows [r, r+32) of a dense block, column groups [g
     int64_t off;            // block offset in the dense array
     int32_t m, r, g0, g1, c0, slot;  // slot: slot index of block row 0 for this column chunk
 };
-struct VItem {              // V rows [q, q+nr) (nr <= 8, one slip) of a block, column groups [g0, g1)
+struct VItem {              // V rows [q, q+nr) (nr <= 32, one slip) of a block, column groups [g0, g1)
     int64_t off;            // block offset in the V array
     int32_t Q, q, nr, g0, g1, c0, s, tp;  // s: slip of these rows; tp: this chunk's partial t (Q values)
 };

@@ -8,8 +8,8 @@
 // A2s x1 + A2d x2, Bs x1 + Bd x2) for c = 0, 1, 2.
 //
 // Work is split into warp items (hm_layout.cuh).  Lanes run over block rows
-// and each lane streams 96 (dense) / 48 (U) / 16 (V) contiguous bytes per
-// column group, so every warp load is a contiguous run of the packed operator.
+// and every warp load instruction reads one contiguous run of the packed
+// operator (512 B for dense and U, four 128 B runs for V).
 // Each dense (block, column chunk) and each low-rank block writes its own
 // per-row partial sums ("slots"); the row reduction adds a row's slots in a
 // fixed order, so results are bitwise reproducible (no atomics).
@@ -82,8 +82,8 @@ template <>
 __device__ __forceinline__ double widen<double, double>(double v) { return v; }
 
 // ------------------------------------------------------------------ kernel 1
-// Dense items (lanes over block rows) and V items (8 rows x 4 column groups per
-// warp load, then a 2-step shuffle reduction per row).
+// Dense items (lanes over block rows) and V items (up to 32 rows: 8 rows x 4
+// column groups per warp load, 4 rows per lane, then a 2-step shuffle reduction).
 template <typename TD, typename TL, typename TA>
 __global__ void __launch_bounds__(256)
 k_dense_v(const DenseItem *__restrict__ ditems, int64_t n_ditems, const VItem *__restrict__ vitems,
@@ -99,8 +99,8 @@ k_dense_v(const DenseItem *__restrict__ ditems, int64_t n_ditems, const VItem *_
         const int r = it.r + lane;
         const bool act = r < it.m;
         TA acc[3] = {0, 0, 0};
-        const TD *p = D + it.off + (int64_t)r * 6 * CWD;
-        const int64_t gstride = (int64_t)it.m * 6 * CWD;
+        const TD *p = D + it.off + (int64_t)r * CWD;           // [group][op][row][CW]
+        const int64_t ostride = (int64_t)it.m * CWD, gstride = 6 * ostride;
         p += (int64_t)it.g0 * gstride;
         const TA *xp = x + 2 * ((int64_t)it.c0 + (int64_t)it.g0 * CWD);   // c0 is CWD-aligned
 #pragma unroll 2
@@ -112,7 +112,7 @@ k_dense_v(const DenseItem *__restrict__ ditems, int64_t n_ditems, const VItem *_
                 for (int c = 0; c < 3; ++c) {
 #pragma unroll
                     for (int s = 0; s < 2; ++s) {
-                        Vec16<TD> d = ld_stream(p + (2 * c + s) * CWD);
+                        Vec16<TD> d = ld_stream(p + (2 * c + s) * ostride);
 #pragma unroll
                         for (int t = 0; t < CWD; ++t) acc[c] += widen<TA>(d.v[t]) * xs[2 * t + s];
                     }
@@ -130,27 +130,37 @@ k_dense_v(const DenseItem *__restrict__ ditems, int64_t n_ditems, const VItem *_
     const int64_t wv = w - n_ditems;
     if (wv >= n_vitems) return;
     const VItem it = vitems[wv];
-    // lane = 8 * jg + rr: row q + rr, column groups g0 + jg, g0 + jg + 4, ...
+    // lane = 8 * jg + rr: rows q + rr + 8u (u < 4), column groups g0 + jg, g0 + jg + 4, ...
+    // Four rows per lane share each x slice.
     const int rr = lane & 7, jg = lane >> 3;
-    TA acc = 0;
+    TA acc[4] = {0, 0, 0, 0};
     if (rr < it.nr) {
         const TL *p = Vd + it.off + ((int64_t)(it.g0 + jg) * it.Q + it.q + rr) * CWV;
         const int64_t gstride = (int64_t)4 * it.Q * CWV;
         const TA *xp = x + (int64_t)(2 + it.s) * xstride + it.c0 + (int64_t)(it.g0 + jg) * CWV;  // CWV-aligned
-#pragma unroll 4
+        const int nu = (it.nr - rr + 7) >> 3;   // rows of this lane (1..4)
+#pragma unroll 2
         for (int g = it.g0 + jg; g < it.g1; g += 4) {
-            Vec16<TL> d = ld_stream(p);
             TA xs[CWV];
             ld_vec<TA, CWV>(xp, xs);
 #pragma unroll
-            for (int t = 0; t < CWV; ++t) acc += widen<TA>(d.v[t]) * xs[t];
+            for (int u = 0; u < 4; ++u) {
+                if (u < nu) {
+                    Vec16<TL> d = ld_stream(p + 8 * u * CWV);
+#pragma unroll
+                    for (int t = 0; t < CWV; ++t) acc[u] += widen<TA>(d.v[t]) * xs[t];
+                }
+            }
             p += gstride;
             xp += 4 * CWV;
         }
     }
-    acc += __shfl_xor_sync(0xffffffffu, acc, 8);
-    acc += __shfl_xor_sync(0xffffffffu, acc, 16);
-    if (jg == 0 && rr < it.nr) tpart[it.tp + it.q + rr] = acc;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], 8);
+        acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], 16);
+        if (jg == 0 && rr + 8 * u < it.nr) tpart[it.tp + it.q + rr + 8 * u] = acc[u];
+    }
 }
 
 // ------------------------------------------------------------------ kernel 2
@@ -202,17 +212,18 @@ k_u(const UTask *__restrict__ tasks, const TL *__restrict__ U, const TA *__restr
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ng = T.K / CW;
-    const int64_t gstride = (int64_t)T.m * 3 * CW;
+    const int64_t gstride = (int64_t)T.m * 3 * CW;   // one column group of U: 3 comps x m rows
     for (int rb = T.r0 + warp * 32; rb < T.r1; rb += blockDim.x) {
         const int r = rb + lane;
         if (r >= T.r1) break;
         TA acc[3] = {0, 0, 0};
-        const TL *p = U + T.off + (int64_t)r * 3 * CW;
+        const TL *p = U + T.off + (int64_t)r * CW;             // [group][comp][row][CW]
+        const int64_t cstride = (int64_t)T.m * CW;
 #pragma unroll 2
         for (int g = 0; g < ng; ++g) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                Vec16<TL> d = ld_stream(p + c * CW);
+                Vec16<TL> d = ld_stream(p + c * cstride);
                 TA tv[CW];
                 smem_vec<TA, CW>(ts + c * T.K + g * CW, tv);
 #pragma unroll

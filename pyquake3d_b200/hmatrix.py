@@ -269,8 +269,8 @@ def build_plan_arrays(struct, dense_recs, kS, kD, code, dense_chunk=64, v_chunk=
             g0 = ch * v_chunk
             g1 = min(ngv, g0 + v_chunk)
             for s_, (qa, qb) in enumerate(((0, 3 * ks), (3 * ks, Q))):
-                for q in range(qa, qb, 8):
-                    vitems.append((v_off, Q, q, min(8, qb - q), g0, g1, b.col.start - lead, s_, tp + ch * Q))
+                for q in range(qa, qb, 32):
+                    vitems.append((v_off, Q, q, min(32, qb - q), g0, g1, b.col.start - lead, s_, tp + ch * Q))
         for r0 in range(0, m, u_rows):
             utasks.append((u_off, m, r0, min(m, r0 + u_rows), K, ks, kd, Q, tp, nch, slot))
         slot_rows.append((slot, b.row.start, m))
@@ -328,8 +328,10 @@ class DeviceHMatrix:
     ("fp64": FP64 everywhere; "fp32": FP32 everywhere; "bf16": FP32 dense,
     BF16 low rank).  matvec(x_dev, dtype) returns y (n x 3, FP64, tree order)."""
 
-    DENSE_CHUNK_GROUPS = 64   # column groups per dense work item
-    V_CHUNK_GROUPS = 64       # column groups per V work item
+    # work-item shapes per storage code (0 FP64, 1 FP32, 2 BF16 low rank), tuned on B200 at 60k
+    DENSE_CHUNK_GROUPS = {0: 64, 1: 16, 2: 16}   # column groups per dense work item
+    V_CHUNK_GROUPS = {0: 128, 1: 32, 2: 32}      # column groups per V work item
+    U_ROWS = 512                                 # rows per U task (one CTA)
 
     def __init__(self, struct, xg, ev, nodes, tri, mu, lam, device="cuda", aca_tol=0.01, aca_rel=False,
                  aca_seed=0, kcap=96, ws_budget_bytes=8 << 30, keep_factors=False):
@@ -498,7 +500,9 @@ class DeviceHMatrix:
         torch = self.torch
         code = DTYPES[dtype]
         kS, kD = self.ranks()
-        A = build_plan_arrays(self.s, self.dense_recs, kS, kD, code, self.DENSE_CHUNK_GROUPS, self.V_CHUNK_GROUPS)
+        pick = lambda v: v[code] if isinstance(v, dict) else v
+        A = build_plan_arrays(self.s, self.dense_recs, kS, kD, code, pick(self.DENSE_CHUNK_GROUPS),
+                              pick(self.V_CHUNK_GROUPS), self.U_ROWS)
         lr_dtype = torch.float64 if code == 0 else (torch.float32 if code == 1 else torch.bfloat16)
         Ubuf = torch.zeros(max(A["u_size"], 8), dtype=lr_dtype, device=self.dev)
         Vbuf = torch.zeros(max(A["v_size"], 8), dtype=lr_dtype, device=self.dev)
@@ -603,9 +607,9 @@ def export_blocks(op):
         m, n, r0, c0 = (int(recs[k][i]) for k in ("m", "n", "r0", "c0"))
         lead = c0 % 2
         ng = _cdiv(n + lead, 2)
-        a = dense[int(recs["off64"][i]):int(recs["off64"][i]) + ng * m * 12].reshape(ng, m, 3, 2, 2)
-        # (group, row, comp, slip, t) -> (slip, comp, row, col)
-        M = a.transpose(3, 2, 1, 0, 4).reshape(2, 3, m, ng * 2)[:, :, :, lead:lead + n].reshape(6, m, n)
+        a = dense[int(recs["off64"][i]):int(recs["off64"][i]) + ng * m * 12].reshape(ng, 3, 2, m, 2)
+        # (group, comp, slip, row, t) -> (slip, comp, row, col)
+        M = a.transpose(2, 1, 3, 0, 4).reshape(2, 3, m, ng * 2)[:, :, :, lead:lead + n].reshape(6, m, n)
         out.append(("dense", perm[r0:r0 + m], perm[c0:c0 + n], np.ascontiguousarray(M)))
     kS, kD = op.ranks()
     u_off = v_off = 0
@@ -622,7 +626,7 @@ def export_blocks(op):
         Q = 3 * (ks + kd)
         lead = b.col.start % 2
         ngv = _cdiv(n + lead, 2)
-        Ub = U[u_off:u_off + K // 2 * m * 6].reshape(K // 2, m, 3, 2).transpose(2, 1, 0, 3).reshape(3, m, K)
+        Ub = U[u_off:u_off + K // 2 * m * 6].reshape(K // 2, 3, m, 2).transpose(1, 2, 0, 3).reshape(3, m, K)
         Vb = V[v_off:v_off + ngv * Q * 2].reshape(ngv, Q, 2).transpose(1, 0, 2).reshape(Q, ngv * 2)[:, lead:lead + n]
         S, D = {}, {}
         for c, (un, vn) in enumerate((("U1", "V1"), ("U2", "V2"), ("UB", "VB"))):

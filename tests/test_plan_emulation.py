@@ -18,11 +18,11 @@ CW_L = {0: 2, 1: 4, 2: 8}
 
 
 def dense_index(m, i, j, c, s, cw):
-    return ((j // cw) * m + i) * (6 * cw) + (2 * c + s) * cw + (j % cw)
+    return (((j // cw) * 6 + 2 * c + s) * m + i) * cw + (j % cw)
 
 
 def u_index(m, i, c, q, cw):
-    return ((q // cw) * m + i) * (3 * cw) + c * cw + (q % cw)
+    return (((q // cw) * 3 + c) * m + i) * cw + (q % cw)
 
 
 def v_index(Q, q, jj, cw):
@@ -98,7 +98,7 @@ def emulate(st, A, D, U, V, x, code):
                 for s in range(2):
                     for t in range(cwd):
                         j = g * cwd + t
-                        acc[:, c] += D[it["off"] + (g * m + rr) * 6 * cwd + (2 * c + s) * cwd + t] * \
+                        acc[:, c] += D[it["off"] + ((g * 6 + 2 * c + s) * m + rr) * cwd + t] * \
                             x[2 * (int(it["c0"]) + j) + s]
         slots[3 * (int(it["slot"]) + rr)[:, None] + np.arange(3)] = acc
     for it in A["vitems"][:A["n_vitems"]]:
@@ -122,7 +122,7 @@ def emulate(st, A, D, U, V, x, code):
         for g in range(K // cwl):
             for c in range(3):
                 for k in range(cwl):
-                    acc[:, c] += U[T["off"] + (g * m + rr) * 3 * cwl + c * cwl + k] * tv[c * K + g * cwl + k]
+                    acc[:, c] += U[T["off"] + ((g * 3 + c) * m + rr) * cwl + k] * tv[c * K + g * cwl + k]
         slots[3 * (int(T["slot"]) + rr)[:, None] + np.arange(3)] = acc
     y = np.zeros((st.n, 3))
     for i in range(st.n):
