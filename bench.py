@@ -2,12 +2,14 @@
 
 Workload ("curved60k"): 150 km rough vertical strike-slip fault + 40 km branch
 at 20 degrees, 59,696 triangles, H-matrix leaf 64, eta 2, ACA relative tol 1e-5;
-operator stored BF16 (low rank) + FP32 (near field), FP64 state and slip;
+operator stored FP32 (BF16 low rank and FP64 also timed), FP64 state and slip;
 reference-mode DP5(4) stepping (one H-matvec per step, frozen load).
 
 A step = one H-matvec of the slip-rate deficit + one fused DP5(4) step kernel
 (accept/reject loop on the device).  The printed JSON line reports:
-  value       steps/s of the mixed-precision path, state resident in HBM
+  value       steps/s of the mixed path (FP32 operator, FP64 state: meets the
+              1e-5 slip target), state resident in HBM; BF16 low rank and FP64
+              plain are timed beside it (all_precisions)
   e2e         steps/s through QDsim.simu_forward (the reference call), with the
               per-step host traffic of the reference main loop (dttry in; h,
               dtnext and max slip rates out; slip-rate and traction vectors out)
@@ -239,6 +241,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--case", default=CASE, help="workload (profiling uses a smaller one)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp64"],
+                    help="operator storage of the headline path (fp32: meets the 1e-5 slip target)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     set_case(args.case)
@@ -264,15 +268,15 @@ def main():
     msh, para = make_case(rank)
     nodes, tris = read_mshV2(msh)
     t0 = time.perf_counter()
-    sim = QDsim(tris, nodes, para, device="cuda:%d" % local, precision="bf16")
+    sim = QDsim(tris, nodes, para, device="cuda:%d" % local, precision=args.precision)
     sim.tree_block.want = ("fp64", "bf16", "fp32")
     t_host = time.perf_counter() - t0
     op = sim.tree_block.op()
     t_asm = time.perf_counter() - t0 - t_host
     kS, kD = op.ranks()
-    mixed = DeviceStepper(sim, op, "bf16")
-    plain = DeviceStepper(sim, op, "fp64")
-    P_m, P_p = op.plan("bf16"), op.plan("fp64")
+    head = args.precision
+    steppers = {p: DeviceStepper(sim, op, p) for p in ("fp32", "bf16", "fp64")}
+    plans = {p: op.plan(p) for p in steppers}
 
     def barrier():
         if world > 1:
@@ -317,25 +321,25 @@ def main():
             raise RuntimeError("step failed with status %d" % int(c[4]))
         return e0.elapsed_time(e1) / 1e3, float(c[0])
 
-    # warm-up (both paths), then the timed mixed-precision region with clock sampling
-    dt_m = dt_p = sim.htry
-    _, dt_m = timed_steps(mixed, args.warmup, dt_m, use_graph=False)
-    _, dt_p = timed_steps(plain, args.warmup, dt_p, use_graph=False)
+    # warm-up of every path, then the timed region of the headline path with clock sampling
+    dts = {}
+    for p, st in steppers.items():
+        _, dts[p] = timed_steps(st, args.warmup, sim.htry, use_graph=False)
+    timing = {}
     clk = Clocks(local)
-    t_mixed, dt_m = timed_steps(mixed, args.steps, dt_m)
+    timing[head], dts[head] = timed_steps(steppers[head], args.steps, dts[head])
     clocks = clk.stop()
-    t_mixed = max_over_ranks(t_mixed)
-    hist_m = mixed.hist.view(-1, 6).cpu().numpy()[:min(args.steps, mixed.hist_cap)]
-    graph_used = id(mixed) in graphs and graphs[id(mixed)] is not None
-    t_plain, dt_p = timed_steps(plain, args.steps, dt_p)
-    t_plain = max_over_ranks(t_plain)
+    hist = steppers[head].hist.view(-1, 6).cpu().numpy()[:min(args.steps, steppers[head].hist_cap)]
+    graph_used = graphs.get(id(steppers[head])) is not None
+    for p in steppers:
+        if p != head:
+            timing[p], dts[p] = timed_steps(steppers[p], args.steps, dts[p])
+    timing = {p: max_over_ranks(t) for p, t in timing.items()}
     steps_total = args.steps * world
-    value = steps_total / t_mixed
+    rate = {p: steps_total / t for p, t in timing.items()}
 
-    # H-matvec alone (the dominant kernel sequence), CUDA events on the launching stream
-    def time_matvec(stepper, P, reps=50):
-        # the operator application as the step runs it (dense/V and U launches; the
-        # per-row sums are folded into the step kernel)
+    # H-matvec alone (k_dense_v + k_u as the step runs them), CUDA events on the launching stream
+    def time_matvec(stepper, reps=50):
         for _ in range(5):
             op.matvec(stepper.x, stepper.precision, slots_only=True)
         torch.cuda.synchronize()
@@ -346,18 +350,19 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / 1e3 / reps
-    t_mv_m = time_matvec(mixed, P_m)
-    t_mv_p = time_matvec(plain, P_p)
     hbm, peak_kind = peaks()
-    gbs_m = P_m["alg_bytes"] / t_mv_m / 1e9
-    gbs_p = P_p["alg_bytes"] / t_mv_p / 1e9
+    mv = {}
+    for p, st in steppers.items():
+        t = time_matvec(st)
+        mv[p] = {"ms": 1e3 * t, "GBs": plans[p]["alg_bytes"] / t / 1e9, "alg_bytes": int(plans[p]["alg_bytes"]),
+                 "frac": plans[p]["alg_bytes"] / t / 1e9 / hbm, "stored_bytes": int(plans[p]["stored_bytes"])}
 
     # accuracy vs the FP64 path at equal times (dt replay of the FP64 run), at several horizons
     accuracy = accuracy_study(sim, op, min(args.steps, 500), precisions=("bf16", "fp32"))
-    slip_err = accuracy["bf16"][-1]["slip"]
 
     # end to end through the reference call surface (QDsim.simu_forward) with the
     # reference main loop's per-step host traffic
+    mixed = steppers[head]
     sim._dev = mixed
     ne = min(args.steps, 300)
     perm_t = torch.as_tensor(op.s.iperm, device=op.dev)
@@ -367,7 +372,7 @@ def main():
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    dttry = dt_m
+    dttry = dts[head]
     for _ in range(ne):
         h, dttry = sim.simu_forward(dttry)
         pin_v.copy_(mixed.t["slipv"].index_select(0, perm_t), non_blocking=True)
@@ -376,7 +381,7 @@ def main():
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
     e2e = {"value": ne * world / t_e2e, "unit": "steps/s", "h2d_bytes_per_step": 8,
-           "d2h_bytes_per_step": int(16 * 8 + 2 * 8 * sim.xg.shape[0]),
+           "d2h_bytes_per_step": int(16 * 8 + 2 * 8 * sim.xg.shape[0]), "steps": ne,
            "path": "QDsim.simu_forward per step + slip-rate and traction vectors to pinned host memory"}
 
     # CPU baseline: the reference's step on the same operator (rank 0, N=1)
@@ -386,9 +391,9 @@ def main():
         from pyquake3d_b200 import QDsim as Q2
         ho = export_host_operator(op)
         host = Q2(tris, nodes, para, device="cuda:0", precision="bf16")
-        rate, k, secs = cpu_reference_steps(ho, qd_oracle.sim_state(host), host.V0, host.mu, host.Cs,
-                                            args.cpu_budget)
-        cpu = {"value": rate, "unit": "steps/s", "cores": 1, "kind": "port",
+        crate, k, secs = cpu_reference_steps(ho, qd_oracle.sim_state(host), host.V0, host.mu, host.Cs,
+                                             args.cpu_budget)
+        cpu = {"value": crate, "unit": "steps/s", "cores": 1, "kind": "port",
                "sample": "%d steps (%.1f s) of the same 60k workload: six block-loop MVMs + DP5(4), "
                          "numpy FP64, one process" % (k, secs)}
         del ho
@@ -397,33 +402,38 @@ def main():
     tp = os.path.join(REPO, "profiles", "hmatvec_traffic.json")
     if os.path.exists(tp):
         try:
-            traffic = json.load(open(tp)).get("bytes_per_matvec_bf16")
+            traffic = json.load(open(tp)).get("bytes_per_matvec_" + head)
         except (ValueError, OSError):
             traffic = None
-    nlaunch_step = (2 if P_m["n_utasks"] > 0 else 1) + 1
+    nlaunch_step = (2 if plans[head]["n_utasks"] > 0 else 1) + 1
+    prec_text = {"fp32": "fp32 operator (near field + low rank), fp64 state and slip",
+                 "bf16": "bf16 low rank / fp32 near field, fp64 state and slip",
+                 "fp64": "fp64 operator and state"}
+    err_head = accuracy.get(head, [{}])[-1] if head in accuracy else {}
     line = {
-        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32 operator, f64 state", "data": "synthetic",
-        "config": {"workload": CASE + " (%d triangles: 150 km rough strike-slip fault + 40 km branch at 20 deg)"
-                               % sim.xg.shape[0],
-                   "precision": "bf16 low-rank / fp32 near-field / fp64 state", "leaf": 64, "eta": 2.0,
-                   "aca": "relative 1e-5", "mean_rank": float(np.mean(np.concatenate([kS, kD]))),
-                   "max_rank": int(max(kS.max(), kD.max())),
-                   "operator_bytes_bf16": int(P_m["stored_bytes"]), "operator_bytes_fp64": int(P_p["stored_bytes"]),
-                   "l2": "inputs larger than L2 (operator %.2f GB per step)" % (P_m["alg_bytes"] / 1e9),
+        "metric": METRIC, "value": rate[head], "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * timing[head] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": {"fp32": "f32 operator, f64 state", "bf16": "bf16+f32 operator, f64 state", "fp64": "f64"}[head],
+        "data": "synthetic",
+        "config": {"workload": CASE + " (%d triangles)" % sim.xg.shape[0], "precision": prec_text[head],
+                   "leaf": int(sim.tree_block.mini_leaf), "eta": 2.0, "aca": "relative 1e-5",
+                   "mean_rank": float(np.mean(np.concatenate([kS, kD]))), "max_rank": int(max(kS.max(), kD.max())),
+                   "l2": "inputs larger than L2 (operator %.2f GB per step)" % (plans[head]["alg_bytes"] / 1e9),
                    "parallelism": "replicas x%d" % world, "host_setup_s": round(t_host, 2),
                    "assembly_s": round(t_asm, 2), "assembly_breakdown": {k: round(v, 3) for k, v in op.timings.items()}},
-        "roofline": {"bound": "hbm", "achieved": gbs_m, "peak": hbm, "unit": "GB/s", "frac": gbs_m / hbm,
-                     "traffic": traffic, "kernel": "H-matvec (k_dense_v + k_u), bf16 low rank / fp32 near field",
-                     "alg_bytes": int(P_m["alg_bytes"]), "ms": 1e3 * t_mv_m, "peak_source": peak_kind},
-        "plain_fp64": {"steps_per_s": steps_total / t_plain, "ms_per_step": 1e3 * t_plain / args.steps,
-                       "hmatvec_GBs": gbs_p, "hmatvec_ms": 1e3 * t_mv_p, "alg_bytes": int(P_p["alg_bytes"]),
-                       "frac": gbs_p / hbm},
-        "mixed_vs_plain": (steps_total / t_mixed) / (steps_total / t_plain),
+        "roofline": {"bound": "hbm", "achieved": mv[head]["GBs"], "peak": hbm, "unit": "GB/s",
+                     "frac": mv[head]["frac"], "traffic": traffic,
+                     "kernel": "H-matvec (k_dense_v + k_u), " + prec_text[head].split(",")[0],
+                     "alg_bytes": mv[head]["alg_bytes"], "ms": mv[head]["ms"], "peak_source": peak_kind},
+        "slip_rel_err_vs_fp64": err_head.get("slip"),
+        "plain_fp64": {"steps_per_s": rate["fp64"], "ms_per_step": 1e3 * timing["fp64"] / args.steps,
+                       "hmatvec": mv["fp64"]},
+        "mixed_vs_plain": rate[head] / rate["fp64"],
+        "all_precisions": {p: {"steps_per_s": rate[p], "ms_per_step": 1e3 * timing[p] / args.steps,
+                               "hmatvec": mv[p], "vs_fp64": rate[p] / rate["fp64"]} for p in steppers},
         "accuracy_vs_fp64": accuracy,
-        "sim": {"time_s": float(hist_m[-1, 2]), "last_dt": float(hist_m[-1, 0]),
-                "rejects": int(hist_m[:, 5].sum())},
+        "sim": {"time_s": float(hist[-1, 2]), "last_dt": float(hist[-1, 0]), "rejects": int(hist[:, 5].sum())},
         "e2e": e2e,
         "cpu_baseline": cpu,
         "gpu_launches": nlaunch_step * args.steps,
@@ -435,7 +445,6 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
-
 
 if __name__ == "__main__":
     main()
