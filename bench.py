@@ -164,6 +164,45 @@ def accuracy_study(sim, op, nrep, precisions=("bf16",), marks=(50, 100, 200, 500
     return out
 
 
+def vmode_study(sim, op, nsteps):
+    """V-mode steps/s with the FP32 and FP64 operators, plain Newton (undamped start)
+    vs the MLP start, and the Newton iteration counts.  The MLP is trained first on
+    solves logged from a short plain run of the same fault."""
+    import torch
+    from pyquake3d_b200.vmode import MLPTrainer, VStepper
+    out = {}
+    logger = VStepper(sim, op, "fp32", seed_mode=1, log_cap=1 << 20)
+    logger.run(20, chunk=4)
+    data = logger.samples()
+    t0 = time.perf_counter()
+    tr = MLPTrainer(seed=0)
+    hist = tr.fit(data, epochs=15, batch=8192, lr=3e-3)
+    torch.cuda.synchronize()
+    out["mlp"] = {"samples": int(data.shape[0]), "epochs": 15, "train_s": round(time.perf_counter() - t0, 2),
+                  "loss_first": hist[0], "loss_last": hist[-1]}
+    del logger
+    for prec, mode in (("fp32", 1), ("fp32", 2), ("fp64", 1)):
+        st = VStepper(sim, op, prec, seed_mode=mode, mlp_params=tr.P if mode == 2 else None)
+        st.run(5, chunk=2)                      # warm-up steps
+        st.reset_stats()
+        c0 = st.ctrl.cpu().numpy().copy()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = st.run(nsteps, chunk=4)
+        e1.record()
+        torch.cuda.synchronize()
+        secs = e0.elapsed_time(e1) / 1e3
+        steps = int(c[8] - c0[8])
+        out["%s_%s" % (prec, "mlp" if mode == 2 else "newton")] = {
+            "steps_per_s": steps / secs, "steps": steps, "attempts": int(c[10] - c0[10]),
+            "matvecs_per_step": 6 * (c[10] - c0[10]) / max(steps, 1), "sim_time_s": float(c[2]),
+            "newton": st.newton_stats()}
+        del st
+    out["mixed_mlp_vs_fp64_newton"] = out["fp32_mlp"]["steps_per_s"] / out["fp64_newton"]["steps_per_s"]
+    return out
+
+
 # --------------------------------------------------------------------- reference arm (CPU)
 _W = {}
 
@@ -241,6 +280,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--case", default=CASE, help="workload (profiling uses a smaller one)")
+    ap.add_argument("--no-vmode", action="store_true", help="skip the V-mode study")
+    ap.add_argument("--vmode-steps", type=int, default=60)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp64"],
                     help="operator storage of the headline path (fp32: meets the 1e-5 slip target)")
     args = ap.parse_args()
@@ -360,6 +401,12 @@ def main():
     # accuracy vs the FP64 path at equal times (dt replay of the FP64 run), at several horizons
     accuracy = accuracy_study(sim, op, min(args.steps, 500), precisions=("bf16", "fp32"))
 
+    # V-mode: DP5(4) with one H-matvec per stage and a Newton solve for V; MLP seed
+    # trained on the run's own solves (hand-written kernels)
+    vmode = None
+    if not args.no_vmode:
+        vmode = vmode_study(sim, op, args.vmode_steps)
+
     # end to end through the reference call surface (QDsim.simu_forward) with the
     # reference main loop's per-step host traffic
     mixed = steppers[head]
@@ -433,6 +480,7 @@ def main():
         "all_precisions": {p: {"steps_per_s": rate[p], "ms_per_step": 1e3 * timing[p] / args.steps,
                                "hmatvec": mv[p], "vs_fp64": rate[p] / rate["fp64"]} for p in steppers},
         "accuracy_vs_fp64": accuracy,
+        "vmode": vmode,
         "sim": {"time_s": float(hist[-1, 2]), "last_dt": float(hist[-1, 0]), "rejects": int(hist[:, 5].sum())},
         "e2e": e2e,
         "cpu_baseline": cpu,

@@ -140,6 +140,27 @@ int pq3d_rk_grid(int n);
  * [9] total rejects, [10] total attempts. */
 int pq3d_rk_step(const void *args, int grid, cudaStream_t stream);
 
+/* ---------------------------------------------------------------- V-mode and MLP
+ * No counterpart in the reference: slip and state integrated with DP5(4), one
+ * H-matvec per stage, the slip rate from a radiation-damped Newton solve per
+ * element seeded by the previous rate, the undamped bound or an MLP
+ * (formulation in pyquake3d_b200/csrc/vmode.cu; parity unpinned by the reference). */
+size_t pq3d_vmode_args_bytes(void);
+int pq3d_vmode_grid(int n);
+/* stage 1..7 after a matvec of that stage's deficit; -1 writes the step-start deficit;
+ * 0 finalizes an attempt (accept/reject decided on the device). */
+int pq3d_vmode_stage(const void *args, int stage, cudaStream_t stream);
+/* 5-64-64-1 tanh MLP, FP32, 4609 parameters: forward, gradient of the mean squared
+ * error, and one Adam step; scratch of pq3d_mlp_scratch_floats(B) floats. */
+int pq3d_mlp_param_count(void);
+int64_t pq3d_mlp_scratch_floats(int B);
+int pq3d_mlp_forward(const float *d_P, const float *d_X, int xstride, int B, float *d_Y, cudaStream_t stream);
+int pq3d_mlp_grad(const float *d_P, const float *d_X, int xstride, const float *d_T, int tstride, int B,
+                  float *d_scratch, float *d_G, float *d_loss, cudaStream_t stream);
+int pq3d_mlp_train_step(float *d_P, float *d_M, float *d_V, const float *d_X, int xstride, const float *d_T,
+                        int tstride, int B, float *d_scratch, float *d_G, float lr, float beta1, float beta2,
+                        float eps, int step, float *d_loss, cudaStream_t stream);
+
 /* No counterpart in the reference.  The same step as pq3d_rk_step for callers
  * that cannot allocate device memory (a host framework that owns every device
  * buffer, an embedded solver handed only its state vectors, a time loop that

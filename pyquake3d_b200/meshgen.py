@@ -231,6 +231,15 @@ def make_case(name, outdir, n_target=None, precision=None):
         cols = friction_layout(xc, 8.0, seed=0, core=(1.0, 6.0))
         return write_case(outdir, name, P, T, cols, leaf=32, tol=0.01, rel=False,
                           precision=precision or "fp64", steps=100)
+    if name == "tinynuc":
+        # tiny fault with a 2 km patch slipping at 1 m/s: radiation damping matters there
+        nx = int(np.sqrt((n_target or 512) / 4.0) * 2)
+        nz = max(2, (n_target or 512) // (2 * nx))
+        P, T = planar(16.0, 8.0, 70.0, nx, nz, jitter=0.1, seed=5)
+        xc = centroids_km(P, T)
+        cols = friction_layout(xc, 8.0, seed=0, core=(1.0, 6.0), nuc=(xc[len(xc) // 2], 2.0, 1.0))
+        return write_case(outdir, name, P, T, cols, leaf=32, tol=0.01, rel=False,
+                          precision=precision or "fp64", steps=100)
     if name == "thrust20k":
         P, T = planar(100.0, 40.0, 30.0, 160, 64, jitter=0.1, seed=1)
         xc = centroids_km(P, T)
