@@ -158,6 +158,7 @@ class HStructure:
         self.n = len(xg)
         self.mini_leaf = mini_leaf
         self.eta = eta
+        self.min_size = min_size
         self.row_root, self.perm, self.leaves = build_cluster_tree(xg, min_size)
         # the reference builds the column tree with the same call: identical tree
         self.col_root = self.row_root
@@ -499,10 +500,7 @@ class DeviceHMatrix:
                                  "assemble(want=...) or construct with keep_factors=True")
         torch = self.torch
         code = DTYPES[dtype]
-        kS, kD = self.ranks()
-        pick = lambda v: v[code] if isinstance(v, dict) else v
-        A = build_plan_arrays(self.s, self.dense_recs, kS, kD, code, pick(self.DENSE_CHUNK_GROUPS),
-                              pick(self.V_CHUNK_GROUPS), self.U_ROWS)
+        A = self.plan_arrays(dtype)
         lr_dtype = torch.float64 if code == 0 else (torch.float32 if code == 1 else torch.bfloat16)
         Ubuf = torch.zeros(max(A["u_size"], 8), dtype=lr_dtype, device=self.dev)
         Vbuf = torch.zeros(max(A["v_size"], 8), dtype=lr_dtype, device=self.dev)
@@ -522,11 +520,33 @@ class DeviceHMatrix:
             check(self.L.pq3d_aca_pack(ptr(d_rec), len(rows), ptr(self.aca_ws[wi][0]), ptr(self.rowlist),
                                        ptr(self.collist), ptr(self.iperm), code, ptr(Ubuf), ptr(Vbuf), self._stream),
                   "pq3d_aca_pack")
+        return self._finish_plan(dtype, A, Ubuf, Vbuf)
+
+    def plan_arrays(self, dtype):
+        """Host work-item arrays of one storage precision (deterministic from the
+        structure and the ACA ranks)."""
+        code = DTYPES[dtype]
+        kS, kD = self.ranks()
+        pick = lambda v: v[code] if isinstance(v, dict) else v
+        return build_plan_arrays(self.s, self.dense_recs, kS, kD, code, pick(self.DENSE_CHUNK_GROUPS),
+                                 pick(self.V_CHUNK_GROUPS), self.U_ROWS)
+
+    def install_plan(self, dtype, Ubuf, Vbuf):
+        """Register a plan whose packed low-rank buffers were produced elsewhere (an
+        operator checkpoint); dense blocks must already be in dense64/dense32."""
+        return self._finish_plan(dtype, self.plan_arrays(dtype), Ubuf, Vbuf)
+
+    def _finish_plan(self, dtype, A, Ubuf, Vbuf):
+        torch = self.torch
+        code = DTYPES[dtype]
 
         def dev_rec(a):
             return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8)).to(self.dev)
 
         acc = torch.float64 if code == 0 else torch.float32
+        dense = self.dense64 if code == 0 else self.dense32
+        if A["n_ditems"] > 0 and dense is None:
+            raise _lib.Pq3dError(f"dense blocks of the {dtype} plan were not assembled")
         P = dict(code=code, dtype=dtype, acc=acc,
                  dense=self.dense64 if code == 0 else self.dense32, U=Ubuf, V=Vbuf,
                  ditems=dev_rec(A["ditems"]), vitems=dev_rec(A["vitems"]), utasks=dev_rec(A["utasks"]),

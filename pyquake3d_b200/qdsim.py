@@ -266,9 +266,21 @@ class QDsim:
         return self.maxsize
 
     def get_block_core(self):
-        """(loaded, blocks): this implementation keeps operators on the device; a saved
-        operator is loaded by pyquake3d_b200.checkpoint, not joblib."""
-        return False, []
+        """(loaded, blocks) as QDsim.get_block_core (src/QDsim.py:199-218).  True when the
+        Corefunc directory holds an operator checkpoint written for this mesh and these
+        parameters (pyquake3d_b200.checkpoint); the operator is then on the device.  A
+        checkpoint of another mesh or parameter set is ignored (False)."""
+        from . import checkpoint
+        os.makedirs(self.Corefunc_directory, exist_ok=True)
+        path = os.path.join(self.Corefunc_directory, checkpoint.FILE_NAME)
+        if not os.path.exists(path):
+            return False, []
+        try:
+            self.tree_block.load(path)
+        except _lib.Pq3dError as e:
+            print("operator checkpoint not used:", e, flush=True)
+            return False, []
+        return True, self.tree_block.blocks_to_process
 
     # ------------------------------------------------------------------ device state
     def _ensure_device(self):
@@ -315,8 +327,11 @@ class BlockTree:
             self.master()
         return self._op
 
-    def master(self, dir=None, blocks_to_process=None, num_workers=None, save_corefunc=False):
-        """Assemble every block on the GPU (dense near field + batched ACA)."""
+    def _want(self):
+        sim = self.sim
+        return getattr(self, "want", None) or (("fp64",) if sim.precision == "fp64" else ("fp64", sim.precision))
+
+    def _new_op(self):
         sim = self.sim
         if sim.halfspace_jud:
             raise _lib.Pq3dError("half-space Green's function is not available in this build")
@@ -324,10 +339,32 @@ class BlockTree:
         tol = float(P.get("ACA tolerance", 0.01))
         rel = P.get("ACA relative tolerance", "False") == "True"
         seed = int(P.get("ACA seed", 0))
-        want = getattr(self, "want", None) or (("fp64",) if sim.precision == "fp64" else ("fp64", sim.precision))
-        self._op = DeviceHMatrix(self.struct, sim.xg, sim.eleVec, sim.nodelst, sim.elelst, sim.mu, sim.lambda_,
-                                 device=sim.device, aca_tol=tol, aca_rel=rel, aca_seed=seed).assemble(want)
+        return DeviceHMatrix(self.struct, sim.xg, sim.eleVec, sim.nodelst, sim.elelst, sim.mu, sim.lambda_,
+                             device=sim.device, aca_tol=tol, aca_rel=rel, aca_seed=seed)
+
+    def master(self, dir=None, blocks_to_process=None, num_workers=None, save_corefunc=False):
+        """Assemble every block on the GPU (dense near field + batched ACA); with
+        save_corefunc, write the operator checkpoint into dir (the reference's
+        blocks_to_process.joblib, src/Hmatrix.py:1240-1241)."""
+        self._op = self._new_op().assemble(self._want())
+        if save_corefunc and dir:
+            from . import checkpoint
+            os.makedirs(dir, exist_ok=True)
+            checkpoint.save_operator(self._op, os.path.join(dir, checkpoint.FILE_NAME), self.sim.xg,
+                                     self.sim.eleVec)
         return self._op
+
+    def load(self, path):
+        """Operator from a checkpoint (every precision the simulation needs must be in it)."""
+        from . import checkpoint
+        header = checkpoint.read_header(path)
+        missing = [d for d in self._want() if d not in header["precisions"]]
+        if missing:
+            raise _lib.Pq3dError(f"checkpoint lacks the {missing} operator(s)")
+        op = self._new_op()
+        checkpoint.load_operator(op, path, self.sim.xg, self.sim.eleVec)
+        self._op = op
+        return op
 
     def worker(self):
         return None

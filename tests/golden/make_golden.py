@@ -21,6 +21,9 @@ What it does:
                         state, block structure, ACA ranks and factors of
                         a few blocks, the six operator products on fixed
                         vectors, and 30 simu_forward steps (seeded ACA starts)
+      output_case.npz   seeded state fields on the tiny mesh and the SHA-256 of
+                        the files QDsim.ouputVTK and QDsim.outputtxt write
+                        for them (output formats, byte for byte)
 The fixtures are small (< 1 MB) and are what the CPU tests pin against.
 """
 import argparse
@@ -223,9 +226,65 @@ def tiny_case(workdir, QDsim_mod, readmsh, Hmatrix):
     return out
 
 
+OUTPUT_FIELDS = ("Tno", "Tt", "Tt1o", "Tt2o", "rake", "state", "slipv", "slipv1", "slipv2", "a", "b", "dc", "fric",
+                 "slip", "slip1", "slip2", "slipvC")
+
+
+def output_fields(nodes, tris, xg, seed=11):
+    """Seeded state of the tiny mesh spanning the magnitudes a run produces."""
+    rng = np.random.default_rng(seed)
+    n = len(tris)
+    f = dict(nodelst=np.asarray(nodes, dtype=np.float64), elelst=np.asarray(tris), xg=np.asarray(xg, dtype=np.float64))
+    f["Tno"] = rng.uniform(20, 80, n)
+    f["Tt1o"] = rng.normal(0, 20, n)
+    f["Tt2o"] = rng.normal(0, 20, n)
+    f["Tt"] = np.sqrt(f["Tt1o"] ** 2 + f["Tt2o"] ** 2)
+    f["rake"] = np.arctan2(f["Tt2o"], f["Tt1o"])
+    f["state"] = rng.uniform(0.5, 0.9, n)
+    f["slipv1"] = 10.0 ** rng.uniform(-14, 0.5, n) * rng.choice([-1, 1], n)
+    f["slipv2"] = 10.0 ** rng.uniform(-14, 0.5, n) * rng.choice([-1, 1], n)
+    f["slipv"] = np.sqrt(f["slipv1"] ** 2 + f["slipv2"] ** 2)
+    f["a"] = rng.uniform(0.005, 0.025, n)
+    f["b"] = rng.uniform(0.01, 0.02, n)
+    f["dc"] = rng.uniform(0.005, 0.05, n)
+    f["fric"] = f["Tt"] / f["Tno"]
+    f["slip1"] = rng.normal(0, 3, n)
+    f["slip2"] = rng.normal(0, 3, n)
+    f["slip"] = np.sqrt(f["slip1"] ** 2 + f["slip2"] ** 2)
+    f["slipvC"] = np.full(n, 1e-9) * rng.uniform(0.5, 1.5, n)
+    f["maxsize"] = 0.9
+    return f
+
+
+def output_case(work, QDsim_mod):
+    import hashlib
+    import types as _types
+    t = np.load(os.path.join(HERE, "tiny_case.npz"))
+    f = output_fields(t["nodes"], t["tris"], t["xg"])
+    obj = _types.SimpleNamespace(**f)
+    out = {k: v for k, v in f.items() if k in OUTPUT_FIELDS}
+    d = os.path.join(work, "outcase")
+    os.makedirs(d)
+    cwd = os.getcwd()
+    os.chdir(d)
+    try:
+        QDsim_mod.QDsim.ouputVTK(obj, "ref.vtk")
+        QDsim_mod.QDsim.outputtxt(obj, "step5")
+        files = ["ref.vtk"] + ["out_txt/" + x for x in sorted(os.listdir("out_txt"))]
+        for fn in files:
+            with open(fn, "rb") as fh:
+                out["sha256:" + fn] = np.array(hashlib.sha256(fh.read()).hexdigest())
+    finally:
+        os.chdir(cwd)
+    out["output_seed"] = 11
+    out["maxsize"] = np.array(f["maxsize"])
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", default=None, help="regenerate one fixture: gf | tiny | output")
     args = ap.parse_args()
     ref_src = os.path.join(args.ref, "src")
     subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref", "REFSRC=" + os.path.join(ref_src, "TDstressFS_C.cpp")],
@@ -244,14 +303,19 @@ def main():
         import Hmatrix
         import QDsim
         lib = ctypes.CDLL(os.path.join(work, "src", "TDstressFS_C.so"))
-        g = gf_cases(lib, SH_greenfunction)
-        np.savez_compressed(os.path.join(HERE, "gf_cases.npz"), **g)
-        t = tiny_case(work, QDsim, readmsh, Hmatrix)
-        np.savez_compressed(os.path.join(HERE, "tiny_case.npz"), **t)
+        if args.only in (None, "gf"):
+            g = gf_cases(lib, SH_greenfunction)
+            np.savez_compressed(os.path.join(HERE, "gf_cases.npz"), **g)
+        if args.only in (None, "tiny"):
+            t = tiny_case(work, QDsim, readmsh, Hmatrix)
+            np.savez_compressed(os.path.join(HERE, "tiny_case.npz"), **t)
+        if args.only in (None, "output"):
+            o = output_case(work, QDsim)
+            np.savez_compressed(os.path.join(HERE, "output_case.npz"), **o)
     finally:
         os.chdir(cwd)
         shutil.rmtree(work, ignore_errors=True)
-    for f in ("gf_cases.npz", "tiny_case.npz"):
+    for f in ("gf_cases.npz", "tiny_case.npz", "output_case.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
 
 
