@@ -140,6 +140,20 @@ int pq3d_rk_grid(int n);
  * [9] total rejects, [10] total attempts. */
 int pq3d_rk_step(const void *args, int grid, cudaStream_t stream);
 
+/* ---------------------------------------------------------------- ensemble
+ * Many independent faults stepped together (the reference runs one fault per
+ * process; this is the batched form of its simu_forward, src/QDsim.py:892-996):
+ * one block-diagonal H-matvec for all faults, then one cooperative launch that
+ * performs, for every fault, the step of pq3d_rk_step with the fault's own
+ * controller.  Rows of a fault are a contiguous tree-order range; CTA tasks of
+ * at most pq3d_ens_task_rows() rows never span two faults.  ctrl holds 16
+ * doubles per fault (layout of the pq3d_rk_step control block), hist 6 doubles
+ * per (step, fault). */
+size_t pq3d_ens_args_bytes(void);
+int pq3d_ens_task_rows(void);
+int pq3d_ens_grid(int n_tasks);
+int pq3d_ens_step(const void *args, int grid, cudaStream_t stream);
+
 /* ---------------------------------------------------------------- V-mode and MLP
  * No counterpart in the reference: slip and state integrated with DP5(4), one
  * H-matvec per stage, the slip rate from a radiation-damped Newton solve per

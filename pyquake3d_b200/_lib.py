@@ -36,6 +36,15 @@ RK_ARGS = np.dtype([(p, "u8") for p in _RK_PTRS] +
                    [("n", "i4"), ("fix_tn", "i4"), ("x_fp32", "i4"), ("step_index", "i4"), ("fuse_rowsum", "i4"),
                     ("slots_fp32", "i4"), ("V0", "f8"), ("eta", "f8"), ("reltol", "f8")], align=True)
 
+_ENS_PTRS = ["Tno", "Tt1o", "Tt2o", "psi", "slip1", "slip2", "slipv1", "slipv2", "slipv", "rake", "Tt", "fric", "slip",
+             "a", "b", "dc", "f0", "shear_loading", "normal_loading", "vplc", "cr0", "sr0",
+             "y", "cand", "x", "slots", "leaf_of_row", "leaf_ptr", "leaf_off", "task_row", "task_fault", "fault_task",
+             "tmax", "ctrl", "fstate", "hist", "hforce", "bar"]
+ENS_ARGS = np.dtype([(p, "u8") for p in _ENS_PTRS] +
+                    [(k, "i4") for k in ("n", "n_faults", "n_tasks", "fix_tn", "x_fp32", "step_index", "fuse_rowsum",
+                                         "slots_fp32")] +
+                    [("V0", "f8"), ("eta", "f8"), ("reltol", "f8")], align=True)
+
 _lib = None
 
 
@@ -87,14 +96,19 @@ def load():
     L.pq3d_rk_args_bytes.restype = ctypes.c_size_t
     L.pq3d_rk_grid.argtypes = [i32]
     L.pq3d_rk_step.argtypes = [vp, i32, vp]
+    L.pq3d_ens_args_bytes.restype = ctypes.c_size_t
+    L.pq3d_ens_grid.argtypes = [i32]
+    L.pq3d_ens_step.argtypes = [vp, i32, vp]
     for f in ("pq3d_src_records", "pq3d_traction_pairs", "pq3d_stress_points", "pq3d_dense_assemble",
-              "pq3d_aca_batched", "pq3d_aca_pack", "pq3d_hmatvec", "pq3d_rk_grid", "pq3d_rk_step"):
+              "pq3d_aca_batched", "pq3d_aca_pack", "pq3d_hmatvec", "pq3d_rk_grid", "pq3d_rk_step", "pq3d_ens_grid",
+              "pq3d_ens_step", "pq3d_ens_task_rows"):
         getattr(L, f).restype = ctypes.c_int
     sizes = {"DenseItem": (L.pq3d_item_bytes(0), DENSE_ITEM.itemsize), "VItem": (L.pq3d_item_bytes(1), V_ITEM.itemsize),
              "UTask": (L.pq3d_item_bytes(2), U_TASK.itemsize),
              "DenseBlock": (L.pq3d_item_bytes(4), DENSE_BLOCK.itemsize), "HmPlan": (L.pq3d_item_bytes(5), HM_PLAN.itemsize),
              "AcaTask": (L.pq3d_aca_task_bytes(), ACA_TASK.itemsize), "PackTask": (L.pq3d_pack_task_bytes(), PACK_TASK.itemsize),
-             "RkArgs": (L.pq3d_rk_args_bytes(), RK_ARGS.itemsize)}
+             "RkArgs": (L.pq3d_rk_args_bytes(), RK_ARGS.itemsize),
+             "EnsArgs": (L.pq3d_ens_args_bytes(), ENS_ARGS.itemsize)}
     bad = {k: v for k, v in sizes.items() if v[0] != v[1]}
     if bad:
         raise Pq3dError(f"record layout mismatch between libpq3d.so and Python: {bad}")

@@ -410,7 +410,9 @@ class DeviceHMatrix:
     def _run_aca(self):
         """Batched ACA over all admissible blocks; ranks and FP64 factors kept per task."""
         torch = self.torch
-        starts = aca_start_indices(self.s.blocks, self.aca_seed)
+        starts = getattr(self.s, "aca_starts", None)
+        if starts is None:
+            starts = aca_start_indices(self.s.blocks, self.aca_seed)
         rowlist, collist = [], []
         tasks = []
         roff = 0

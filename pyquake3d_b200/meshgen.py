@@ -216,6 +216,35 @@ def write_case(outdir, name, P, T, cols, leaf, tol, rel, precision, steps):
     return msh, para
 
 
+def ensemble_faults(outdir, n_faults=32, seed=4, lo=2000, hi=20000, edge=0.5, precision="fp32", steps=2000):
+    """Batch of independent planar faults of uneven size: N ~ U[lo, hi] triangles
+    (seeded), dip ~ U[20, 90] degrees, length = 2 x width, edge ~`edge` km, 10% node
+    jitter; velocity weakening a in the core drawn from a seeded smooth random
+    field in [0.008, 0.012] (b = 0.015), a = 0.025 elsewhere.  Each fault gets its
+    own directory (mesh, 10-column parameter file, parameter.txt); returns the
+    list of (msh, parameter.txt)."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(lo, hi + 1, n_faults)
+    dips = rng.uniform(20.0, 90.0, n_faults)
+    out = []
+    for f in range(n_faults):
+        nz = max(2, int(round(np.sqrt(sizes[f] / 4.0))))
+        nx = 2 * nz
+        width, length = nz * edge, nx * edge
+        P, T = planar(length, width, float(dips[f]), nx, nz, jitter=0.1, seed=seed * 1000 + f)
+        xc = centroids_km(P, T)
+        depth = -xc[:, 2]
+        core = (depth >= 0.1 * width * np.sin(np.deg2rad(dips[f]))) & \
+               (depth <= 0.8 * width * np.sin(np.deg2rad(dips[f]))) & (np.abs(xc[:, 0]) <= 0.4 * length)
+        cols = friction_layout(xc, length / 2, seed=seed * 1000 + f, vw_patch=lambda c: core)
+        cols[core, 1] = gaussian_field(xc[core], max(2.0, width / 4), seed=seed * 1000 + f + 500, lo=0.008, hi=0.012) \
+            if core.sum() > 1 else 0.010
+        d = os.path.join(outdir, "fault%02d" % f)
+        out.append(write_case(d, "fault%02d" % f, P, T, cols, leaf=64, tol=1e-5, rel=True, precision=precision,
+                              steps=steps))
+    return out
+
+
 def make_case(name, outdir, n_target=None, precision=None):
     """Write one of the named cases; returns (msh_path, parameter_path)."""
     if name == "plain2k":
