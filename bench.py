@@ -207,6 +207,84 @@ def vmode_study(sim, op, nsteps):
 _W = {}
 
 
+def ensemble_study(nsteps, nrep, faults=32):
+    """Batched ensemble: `faults` independent planar faults of uneven size (seeded
+    U[2000, 20000] triangles, dips U[20, 90] degrees, seeded friction), one
+    block-diagonal matvec and one cooperative step launch per step for all.
+    Aggregate fault-steps/s for the FP32 and FP64 operators, matvec bandwidth, and
+    per-fault slip error of the FP32 run against the FP64 run on the FP64 step
+    sizes (dt replay)."""
+    import torch
+    from pyquake3d_b200 import QDsim, read_mshV2
+    from pyquake3d_b200.ensemble import Ensemble
+    from pyquake3d_b200.meshgen import ensemble_faults
+    d = os.path.join(tempfile.gettempdir(), "pq3d_bench_ensemble%d" % faults)
+    if not os.path.exists(os.path.join(d, "fault%02d" % (faults - 1), "parameter.txt")):
+        ensemble_faults(d, n_faults=faults, seed=4, lo=2000, hi=20000, edge=0.5)
+    t0 = time.perf_counter()
+    sims = []
+    for f in range(faults):
+        fd = os.path.join(d, "fault%02d" % f)
+        nodes, tris = read_mshV2(os.path.join(fd, "fault%02d.msh" % f))
+        sims.append(QDsim(tris, nodes, os.path.join(fd, "parameter.txt"), precision="fp32"))
+    t_host = time.perf_counter() - t0
+    E64 = Ensemble(sims, precision="fp64", want=("fp64", "fp32"))
+    torch.cuda.synchronize()
+    t_asm = time.perf_counter() - t0 - t_host
+    E32 = Ensemble(sims, precision="fp32", share=E64)
+    hbm, _ = peaks()
+    out = {"faults": faults, "triangles": int(E64.n), "sizes": [int(s) for s in E64.struct.sizes],
+           "host_setup_s": round(t_host, 2), "assembly_s": round(t_asm, 2)}
+    h0 = [s.htry for s in sims]
+    G = 50
+    for name, E in (("fp32", E32), ("fp64", E64)):
+        E.run(5, h0)                                  # warm-up (and the first steps of the run)
+        E.set_history(G)
+        g = E.capture(G)
+        reps = max(1, nsteps // G)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        E._status()
+        t = e0.elapsed_time(e1) / 1e3
+        P = E.op.plan(name)
+        for _ in range(3):
+            E.op.matvec(E.x, name, slots_only=True)
+        torch.cuda.synchronize()
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record()
+        for _ in range(20):
+            E.op.matvec(E.x, name, slots_only=True)
+        m1.record()
+        torch.cuda.synchronize()
+        tm = m0.elapsed_time(m1) / 1e3 / 20
+        out[name] = {"ensemble_steps_per_s": reps * G / t, "fault_steps_per_s": faults * reps * G / t,
+                     "ms_per_step": 1e3 * t / (reps * G), "steps": reps * G,
+                     "hmatvec": {"ms": 1e3 * tm, "GBs": P["alg_bytes"] / tm / 1e9, "frac": P["alg_bytes"] / tm / 1e9 / hbm,
+                                 "alg_bytes": int(P["alg_bytes"])}}
+        del g
+    out["fp32_vs_fp64"] = out["fp32"]["fault_steps_per_s"] / out["fp64"]["fault_steps_per_s"]
+    # per-fault error: fresh ensembles from the initial state, FP32 on the FP64 step sizes
+    R64 = Ensemble(sims, precision="fp64", share=E64)
+    R32 = Ensemble(sims, precision="fp32", share=E64)
+    h = R64.run(nrep, h0)
+    R32.set_replay(torch.tensor(h[:, :, 0], device=R32.op.dev))
+    R32.run(nrep, h0)
+    errs = []
+    for f in range(faults):
+        a, b = R32.get("slip", f), R64.get("slip", f)
+        errs.append(float(np.linalg.norm(a - b) / np.linalg.norm(b)))
+    out["slip_rel_err_vs_fp64"] = {"steps": nrep, "max": max(errs), "median": float(np.median(errs)),
+                                   "per_fault": errs, "method": "dt replay of the FP64 ensemble"}
+    del E32, E64, R32, R64
+    torch.cuda.empty_cache()
+    return out
+
+
 def _worker_init(blocks):
     _W["blocks"] = blocks
 
@@ -282,6 +360,8 @@ def main():
     ap.add_argument("--case", default=CASE, help="workload (profiling uses a smaller one)")
     ap.add_argument("--no-vmode", action="store_true", help="skip the V-mode study")
     ap.add_argument("--vmode-steps", type=int, default=60)
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 32-fault ensemble study")
+    ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp64"],
                     help="operator storage of the headline path (fp32: meets the 1e-5 slip target)")
     args = ap.parse_args()
@@ -407,6 +487,11 @@ def main():
     if not args.no_vmode:
         vmode = vmode_study(sim, op, args.vmode_steps)
 
+    # batched ensemble of 32 independent faults (one launch per step for all)
+    ensemble = None
+    if not args.no_ensemble and world == 1:
+        ensemble = ensemble_study(args.ensemble_steps, 200)
+
     # end to end through the reference call surface (QDsim.simu_forward) with the
     # reference main loop's per-step host traffic
     mixed = steppers[head]
@@ -481,6 +566,7 @@ def main():
                                "hmatvec": mv[p], "vs_fp64": rate[p] / rate["fp64"]} for p in steppers},
         "accuracy_vs_fp64": accuracy,
         "vmode": vmode,
+        "ensemble": ensemble,
         "sim": {"time_s": float(hist[-1, 2]), "last_dt": float(hist[-1, 0]), "rejects": int(hist[:, 5].sum())},
         "e2e": e2e,
         "cpu_baseline": cpu,

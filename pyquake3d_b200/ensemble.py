@@ -99,7 +99,10 @@ class Ensemble:
     FIELDS = ["Tno", "Tt1o", "Tt2o", "psi", "slip1", "slip2", "slipv1", "slipv2", "slipv", "rake", "Tt", "fric", "slip"]
     CONST = ["a", "b", "dc", "f0", "shear_loading", "normal_loading", "vplc", "cr0", "sr0"]
 
-    def __init__(self, sims, precision="fp32", want=None, device="cuda"):
+    def __init__(self, sims, precision="fp32", want=None, device="cuda", share=None):
+        """sims: host-initialized QDsim objects of the faults.  share: another Ensemble
+        of the same faults whose assembled operator is reused (its plans must
+        include `precision`)."""
         import torch
         self.torch = torch
         self.L = _lib.load()
@@ -113,18 +116,23 @@ class Ensemble:
             if same != (s0.mu, s0.lambda_, s0.V0, s0.Cs, s0.RelTol, bool(s0.fix_Tn)):
                 raise _lib.Pq3dError("ensemble faults must share elastic constants, V0, RelTol and Fix_Tn")
         P = s0.Para0
-        seeds = [int(s.Para0.get("ACA seed", 0)) for s in self.sims]
-        self.struct = EnsembleStructure([s.tree_block.struct for s in self.sims], seeds)
-        xg = np.concatenate([s.xg for s in self.sims])
-        ev = np.concatenate([s.eleVec for s in self.sims])
-        noff = np.concatenate([[0], np.cumsum([len(s.nodelst) for s in self.sims])])
-        nodes = np.concatenate([s.nodelst for s in self.sims])
-        tri = np.concatenate([np.asarray(s.elelst) + o for s, o in zip(self.sims, noff)])
-        tol = float(P.get("ACA tolerance", 0.01))
-        rel = P.get("ACA relative tolerance", "False") == "True"
-        want = tuple(want or (("fp64",) if precision == "fp64" else ("fp64", precision)))
-        self.op = DeviceHMatrix(self.struct, xg, ev, nodes, tri, s0.mu, s0.lambda_, device=device, aca_tol=tol,
-                                aca_rel=rel).assemble(want)
+        if share is not None:
+            if len(share.sims) != len(self.sims):
+                raise _lib.Pq3dError("shared ensemble has another number of faults")
+            self.struct, self.op = share.struct, share.op
+        else:
+            seeds = [int(s.Para0.get("ACA seed", 0)) for s in self.sims]
+            self.struct = EnsembleStructure([s.tree_block.struct for s in self.sims], seeds)
+            xg = np.concatenate([s.xg for s in self.sims])
+            ev = np.concatenate([s.eleVec for s in self.sims])
+            noff = np.concatenate([[0], np.cumsum([len(s.nodelst) for s in self.sims])])
+            nodes = np.concatenate([s.nodelst for s in self.sims])
+            tri = np.concatenate([np.asarray(s.elelst) + o for s, o in zip(self.sims, noff)])
+            tol = float(P.get("ACA tolerance", 0.01))
+            rel = P.get("ACA relative tolerance", "False") == "True"
+            want = tuple(want or (("fp64",) if precision == "fp64" else ("fp64", precision)))
+            self.op = DeviceHMatrix(self.struct, xg, ev, nodes, tri, s0.mu, s0.lambda_, device=device, aca_tol=tol,
+                                    aca_rel=rel).assemble(want)
         self.n = n = self.struct.n
         self.M = M = self.struct.faults
         self.perm = self.struct.perm
