@@ -140,6 +140,19 @@ int pq3d_rk_grid(int n);
  * [9] total rejects, [10] total attempts. */
 int pq3d_rk_step(const void *args, int grid, cudaStream_t stream);
 
+/* Row-partitioned step (one fault over several GPUs, each rank owning tree-order
+ * rows [r0, r1); replaces the reference's MPI block split with its reduce of the
+ * products, src/QDsim.py:906-922).  Plain launches on the rank's rows; the host
+ * reduces the returned maxima over ranks and applies the controller.
+ * attempt: one DP5(4) attempt of size h (first = 1 also sums the matvec slots
+ * into y); d_out[8] = error maxima (psi, Tt1, Tt2, Tno) with NaN -> 0, then NaN
+ * flags.  accept: the accepted-step update of the rows, the rows' deficit into
+ * args.x; d_out[0..1] = max|V1|, max|V2|.  args.blk: 4 * grid doubles;
+ * args.bar[2] zero before the first call (the kernels leave it zero). */
+int pq3d_rk_rows_attempt(const void *args, int grid, int r0, int r1, double h, int first, double *d_out,
+                         cudaStream_t stream);
+int pq3d_rk_rows_accept(const void *args, int grid, int r0, int r1, double h, double *d_out, cudaStream_t stream);
+
 /* ---------------------------------------------------------------- ensemble
  * Many independent faults stepped together (the reference runs one fault per
  * process; this is the batched form of its simu_forward, src/QDsim.py:892-996):

@@ -293,7 +293,9 @@ class OracleStepper:
         dtau2dt = (-self.AdotV2 + self.shear_loading - eta * (dV2dsigma * self.dsigmadt + dV2dstate * dstatedt)) / (1.0 + eta * dV2dtau)
         return dstatedt, self.dsigmadt / 1e6, dtau1dt / 1e6, dtau2dt / 1e6
 
-    def rk(self, h):
+    def rk_stages(self, h):
+        """The seven DP5(4) stages (src/QDsim.py:1001-1134): (y5, y8), each the
+        tuple (Tno, Tt1o, Tt2o, psi) of element arrays."""
         B21 = .2
         B31, B32 = 3. / 40, 9. / 40.
         B41, B42, B43 = 44. / 45., -56. / 15, 32. / 9
@@ -323,6 +325,11 @@ class OracleStepper:
         y8 = tuple(y0[q] + h * (B81 * k1[q] + B83 * k3[q] + B84 * k4[q] + B85 * k5[q] + B86 * k6[q] + B87 * k7[q])
                    for q in range(4))
         del order
+        return y5, y8
+
+    def rk(self, h):
+        """One attempt: 5th-order candidate, error ratios and proposed steps."""
+        y5, y8 = self.rk_stages(h)
         err = tuple(np.abs(y8[q] - y5[q]) for q in range(4))
         R1 = np.max(np.abs(err[3] / y8[3])) + 1e-10
         R2 = max(np.max(np.abs(err[1] / y8[1])), np.max(np.abs(err[2] / y8[2])), np.max(np.abs(err[0] / y8[0]))) + 1e-10

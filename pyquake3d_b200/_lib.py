@@ -96,12 +96,14 @@ def load():
     L.pq3d_rk_args_bytes.restype = ctypes.c_size_t
     L.pq3d_rk_grid.argtypes = [i32]
     L.pq3d_rk_step.argtypes = [vp, i32, vp]
+    L.pq3d_rk_rows_attempt.argtypes = [vp, i32, i32, i32, ctypes.c_double, i32, vp, vp]
+    L.pq3d_rk_rows_accept.argtypes = [vp, i32, i32, i32, ctypes.c_double, vp, vp]
     L.pq3d_ens_args_bytes.restype = ctypes.c_size_t
     L.pq3d_ens_grid.argtypes = [i32]
     L.pq3d_ens_step.argtypes = [vp, i32, vp]
     for f in ("pq3d_src_records", "pq3d_traction_pairs", "pq3d_stress_points", "pq3d_dense_assemble",
               "pq3d_aca_batched", "pq3d_aca_pack", "pq3d_hmatvec", "pq3d_rk_grid", "pq3d_rk_step", "pq3d_ens_grid",
-              "pq3d_ens_step", "pq3d_ens_task_rows"):
+              "pq3d_ens_step", "pq3d_ens_task_rows", "pq3d_rk_rows_attempt", "pq3d_rk_rows_accept"):
         getattr(L, f).restype = ctypes.c_int
     sizes = {"DenseItem": (L.pq3d_item_bytes(0), DENSE_ITEM.itemsize), "VItem": (L.pq3d_item_bytes(1), V_ITEM.itemsize),
              "UTask": (L.pq3d_item_bytes(2), U_TASK.itemsize),

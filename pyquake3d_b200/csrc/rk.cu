@@ -222,6 +222,74 @@ __global__ void __launch_bounds__(RK_THREADS) k_rk_step(RkArgs A)
     }
 }
 
+// Row-range kernels of the row-partitioned (multi-GPU) step: the same element
+// work as k_rk_step on rows [r0, r1) only, as plain launches; the host applies
+// the controller to maxima reduced over all ranks.  Per-CTA maxima go to blk;
+// the last CTA to finish (bar[2] count, no waiting) reduces them into out:
+// out[0..4) values with NaN replaced by 0, out[4..8) NaN flags.
+template <int NT>
+__device__ void rows_finish(const RkArgs &A, double *v, double *out)
+{
+    __shared__ double wred[NT / 32][4];
+    __shared__ int s_done;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] = nanmax(v[q], __shfl_down_sync(0xffffffffu, v[q], o));
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) wred[threadIdx.x >> 5][q] = v[q];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < 4; ++q) {
+            double w = wred[0][q];
+            for (int k = 1; k < NT / 32; ++k) w = nanmax(w, wred[k][q]);
+            A.blk[(int64_t)q * gridDim.x + blockIdx.x] = w;
+        }
+        __threadfence();
+        s_done = atomicAdd(A.bar + 2, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_done || threadIdx.x != 0) return;
+    __threadfence();
+    for (int q = 0; q < 4; ++q) {
+        double w = 0.0;
+        for (unsigned k = 0; k < gridDim.x; ++k) w = nanmax(w, __ldcg(A.blk + (int64_t)q * gridDim.x + k));
+        const bool isnan_w = w != w;
+        out[q] = isnan_w ? 0.0 : w;
+        out[4 + q] = isnan_w ? 1.0 : 0.0;
+    }
+    A.bar[2] = 0u;
+}
+
+__global__ void __launch_bounds__(RK_THREADS) k_rk_rows_attempt(RkArgs A, int r0, int r1, double h, int first,
+                                                                double *out)
+{
+    double e4[4] = {0.0, 0.0, 0.0, 0.0};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < r1; i += stride) {
+        if (first && A.fuse_rowsum) fused_rowsum(A, i);
+        double e[4];
+        dp54_element(A, i, h, e);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) e4[q] = nanmax(e4[q], e[q]);
+    }
+    rows_finish<RK_THREADS>(A, e4, out);
+}
+
+__global__ void __launch_bounds__(RK_THREADS) k_rk_rows_accept(RkArgs A, int r0, int r1, double h, double *out)
+{
+    double v4[4] = {0.0, 0.0, 0.0, 0.0};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < r1; i += stride) {
+        double v1, v2;
+        accept_element(A, i, h, v1, v2);
+        v4[0] = fmax(v4[0], fabs(v1));
+        v4[1] = fmax(v4[1], fabs(v2));
+    }
+    rows_finish<RK_THREADS>(A, v4, out);
+}
+
 }  // namespace
 
 PQ3D_EXPORT size_t pq3d_rk_args_bytes(void) { return sizeof(RkArgs); }
@@ -236,6 +304,40 @@ PQ3D_EXPORT int pq3d_rk_grid(int n)
     int need = (n + RK_THREADS - 1) / RK_THREADS;
     int cap = sms * per;
     return need < cap ? need : cap;
+}
+
+static int rows_check(const RkArgs &A, int grid, int r0, int r1, const double *out)
+{
+    if (grid <= 0 || r0 < 0 || r1 < r0 || r1 > A.n || !out || !A.blk || !A.bar || !A.cand || !A.y || !A.x) return PQ3D_ERR_ARG;
+    return PQ3D_OK;
+}
+
+// One DP5(4) attempt of size h on rows [r0, r1) (row-partitioned step); out: 8
+// doubles (error maxima psi, Tt1, Tt2, Tno with NaN -> 0, then NaN flags).  blk
+// must hold 4 * grid doubles; bar[2] must be zero before the first call.
+PQ3D_EXPORT int pq3d_rk_rows_attempt(const void *args, int grid, int r0, int r1, double h, int first, double *d_out,
+                                     cudaStream_t stream)
+{
+    if (!args) return PQ3D_ERR_ARG;
+    const RkArgs A = *(const RkArgs *)args;
+    const int rc = rows_check(A, grid, r0, r1, d_out);
+    if (rc != PQ3D_OK) return rc;
+    if (first && A.fuse_rowsum && (!A.slots || !A.leaf_of_row || !A.leaf_ptr || !A.leaf_off)) return PQ3D_ERR_ARG;
+    k_rk_rows_attempt<<<grid, RK_THREADS, 0, stream>>>(A, r0, r1, h, first, d_out);
+    return pq3d_launch_status();
+}
+
+// Accepted step of size h on rows [r0, r1): state, slip, and the rows' deficit in
+// args.x; out[0], out[1] = max |V1|, max |V2| over the rows.
+PQ3D_EXPORT int pq3d_rk_rows_accept(const void *args, int grid, int r0, int r1, double h, double *d_out,
+                                    cudaStream_t stream)
+{
+    if (!args) return PQ3D_ERR_ARG;
+    const RkArgs A = *(const RkArgs *)args;
+    const int rc = rows_check(A, grid, r0, r1, d_out);
+    if (rc != PQ3D_OK) return rc;
+    k_rk_rows_accept<<<grid, RK_THREADS, 0, stream>>>(A, r0, r1, h, d_out);
+    return pq3d_launch_status();
 }
 
 // One reference-mode step.  args: host copy of RkArgs; grid from pq3d_rk_grid.

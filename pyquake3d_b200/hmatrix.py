@@ -255,8 +255,9 @@ def build_plan_arrays(struct, dense_recs, kS, kD, code, dense_chunk=64, v_chunk=
     kmax = 0
     for bi, b in enumerate(aca_blocks):
         m, nn = len(b.row.indices), len(b.col.indices)
+        lo, hi = getattr(b, "rows", (0, m))      # block-local rows this plan computes (all, unless clipped)
         ks, kd = int(kS[bi]), int(kD[bi])
-        lr_entries += 3 * (ks + kd) * (m + nn)
+        lr_entries += 3 * (ks + kd) * ((hi - lo) + nn)
         if ks + kd == 0:
             continue
         K = _cdiv(ks + kd, cwl) * cwl
@@ -272,12 +273,13 @@ def build_plan_arrays(struct, dense_recs, kS, kD, code, dense_chunk=64, v_chunk=
             for s_, (qa, qb) in enumerate(((0, 3 * ks), (3 * ks, Q))):
                 for q in range(qa, qb, 32):
                     vitems.append((v_off, Q, q, min(32, qb - q), g0, g1, b.col.start - lead, s_, tp + ch * Q))
-        for r0 in range(0, m, u_rows):
-            utasks.append((u_off, m, r0, min(m, r0 + u_rows), K, ks, kd, Q, tp, nch, slot))
-        slot_rows.append((slot, b.row.start, m))
+        # row r of the block writes slot (slot - lo) + r, for r in [lo, hi)
+        for r0 in range(lo, hi, u_rows):
+            utasks.append((u_off, m, r0, min(hi, r0 + u_rows), K, ks, kd, Q, tp, nch, slot - lo))
+        slot_rows.append((slot, b.row.start + lo, hi - lo))
         for p in (0, 1):
             pack.append((bi, p, u_off, v_off, K, Q, ks, kd))
-        slot += m
+        slot += hi - lo
         tp += nch * Q
         u_off += (K // cwl) * m * 3 * cwl
         v_off += Q * npad
