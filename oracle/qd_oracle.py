@@ -40,6 +40,8 @@ def td_lib():
         D = ctypes.POINTER(ctypes.c_double)
         L.td_stress_fs_batch.argtypes = [D, D, D, ctypes.c_size_t, D, D, D] + [ctypes.c_double] * 5 + [D, D]
         L.td_stress_each_source.argtypes = [ctypes.c_double] * 3 + [D, D, D, ctypes.c_size_t] + [ctypes.c_double] * 5 + [D, D]
+        L.td_stress_hs_batch.argtypes = [D, D, D, ctypes.c_size_t, D, D, D] + [ctypes.c_double] * 5 + \
+            [ctypes.c_int, D, D]
         L.td_traction_block.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
                                                                  ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                                                  ctypes.c_void_p]
@@ -60,6 +62,20 @@ def td_stress_fs(X, Y, Z, P1, P2, P3, Ss, Ds, Ts, mu, lam):
     L.td_stress_fs_batch(_p(X), _p(Y), _p(Z), n, _p(np.ascontiguousarray(P1, dtype=np.float64)),
                          _p(np.ascontiguousarray(P2, dtype=np.float64)), _p(np.ascontiguousarray(P3, dtype=np.float64)),
                          Ss, Ds, Ts, mu, lam, _p(s), _p(e))
+    return s.reshape(n, 6), e.reshape(n, 6)
+
+
+def td_stress_hs(X, Y, Z, P1, P2, P3, Ss, Ds, Ts, mu, lam, mode=2):
+    """Half-space stress, strain (n x 6), TDstressHS (src/TDstressFS_C.cpp:1911-2000);
+    mode 2 follows the compiled C++ path, mode 1 the numpy twin (they differ only
+    for a triangle side along z that is not the first side)."""
+    L = td_lib()
+    X, Y, Z = (np.ascontiguousarray(v, dtype=np.float64) for v in (X, Y, Z))
+    n = len(X)
+    s, e = np.zeros(6 * n), np.zeros(6 * n)
+    L.td_stress_hs_batch(_p(X), _p(Y), _p(Z), n, _p(np.ascontiguousarray(P1, dtype=np.float64)),
+                         _p(np.ascontiguousarray(P2, dtype=np.float64)), _p(np.ascontiguousarray(P3, dtype=np.float64)),
+                         Ss, Ds, Ts, mu, lam, int(mode), _p(s), _p(e))
     return s.reshape(n, 6), e.reshape(n, 6)
 
 

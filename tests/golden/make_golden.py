@@ -21,6 +21,12 @@ What it does:
                         state, block structure, ACA ranks and factors of
                         a few blocks, the six operator products on fixed
                         vectors, and 30 simu_forward steps (seeded ACA starts)
+      hs_cases.npz      half-space stress/strain of TDstressFS_C with jud_halfspace
+                        (the C++ path the reference's ACA rows/columns use) and of
+                        SH_greenfunction.TDstressHS (the numpy path its dense
+                        blocks use) for triangles at depth, touching the free
+                        surface, with a vertical side and vertical; receivers at
+                        depth, near and on the surface
       output_case.npz   seeded state fields on the tiny mesh and the SHA-256 of
                         the files QDsim.ouputVTK and QDsim.outputtxt write
                         for them (output formats, byte for byte)
@@ -226,6 +232,77 @@ def tiny_case(workdir, QDsim_mod, readmsh, Hmatrix):
     return out
 
 
+def hs_cases(lib, SH):
+    """Half-space fixtures (see the module docstring)."""
+    import ctypes
+    D = ctypes.POINTER(ctypes.c_double)
+    lib.TDstressFS_C.argtypes = [D, D, D, ctypes.c_size_t, D, D, D] + [ctypes.c_double] * 5 + [ctypes.c_bool, D, D]
+    lib.TDstressEachSourceAtReceiver_C.argtypes = [ctypes.c_double] * 3 + [D, D, D, ctypes.c_size_t] + \
+        [ctypes.c_double] * 5 + [ctypes.c_bool, D, D]
+    p = lambda a: a.ctypes.data_as(D)
+    mu = lam = 32038120320.0
+    rng = np.random.default_rng(2024)
+    tris, kinds = [], []
+    for t in range(8):                          # at depth
+        c = np.array([rng.uniform(-5e3, 5e3), rng.uniform(-5e3, 5e3), rng.uniform(-15e3, -3e3)])
+        tris.append(c + rng.normal(size=(3, 3)) * 1500.0)
+        kinds.append("deep")
+    for k, nz in enumerate((1, 2, 2)):          # one or two vertices on the free surface z = 0
+        c = np.array([rng.uniform(-3e3, 3e3), rng.uniform(-3e3, 3e3), -2e3])
+        P = c + rng.normal(size=(3, 3)) * 1500.0
+        P[:, 2] = -np.abs(P[:, 2])
+        P[:nz, 2] = 0.0
+        tris.append(P)
+        kinds.append("surface%d_%d" % (nz, k))
+    # a side along z (P1 -> P2 vertical) and a vertical triangle without vertical sides
+    tris.append(np.array([[1000.0, 500.0, -3000.0], [1000.0, 500.0, -6000.0], [3500.0, 1500.0, -4500.0]]))
+    kinds.append("vertical_side")
+    tris.append(np.array([[-2000.0, 1000.0, -2500.0], [2500.0, 1000.0, -4000.0], [300.0, 1000.0, -7000.0]]))
+    kinds.append("vertical")
+    # the vertical side as the second and third side of the triangle
+    base = tris[-2]
+    tris.append(base[[2, 0, 1]].copy())
+    kinds.append("vertical_side2")
+    tris.append(base[[1, 2, 0]].copy())
+    kinds.append("vertical_side3")
+    tris = np.array(tris)
+    recs = []
+    for P in tris:
+        c = P.mean(axis=0)
+        R = c + rng.normal(size=(80, 3)) * 4000.0
+        R[:, 2] = -np.abs(R[:, 2])
+        R[:10, 2] = -rng.uniform(0.5, 20.0, 10)       # near the surface
+        R[10:16, 2] = 0.0                                # on the surface
+        recs.append(R)
+    recs = np.array(recs)
+    out = {"hs_P": tris, "hs_R": recs, "hs_kind": np.array(kinds), "mu": mu, "lam": lam}
+    for Ss, Ds, Ts, tag in ((1.0, 0.0, 0.0, "ss"), (0.0, 1.0, 0.0, "ds"), (0.7, -0.4, 0.25, "mix")):
+        S = np.zeros(recs.shape[:2] + (6,))
+        E = np.zeros_like(S)
+        N = np.full_like(S, np.nan)
+        for t in range(len(tris)):
+            R = np.ascontiguousarray(recs[t])
+            n = len(R)
+            s, e = np.zeros(6 * n), np.zeros(6 * n)
+            x, y, z = (np.ascontiguousarray(R[:, k]) for k in range(3))
+            lib.TDstressFS_C(p(x), p(y), p(z), n, p(tris[t, 0].copy()), p(tris[t, 1].copy()), p(tris[t, 2].copy()),
+                             Ss, Ds, Ts, mu, lam, True, p(s), p(e))
+            S[t], E[t] = s.reshape(n, 6), e.reshape(n, 6)
+            st, _ = SH.TDstressHS(x.copy(), y.copy(), z.copy(), tris[t, 0].copy(), tris[t, 1].copy(),
+                                  tris[t, 2].copy(), Ss, Ds, Ts, mu, lam)
+            N[t] = np.asarray(st).T
+        out["hs_%s_stress" % tag], out["hs_%s_strain" % tag], out["hs_%s_numpy" % tag] = S, E, N
+    # one receiver, all sources
+    r = np.array([400.0, -300.0, -2500.0])
+    P1f, P2f, P3f = (np.ascontiguousarray(tris[:, k].ravel()) for k in range(3))
+    n = len(tris)
+    s, e = np.zeros(6 * n), np.zeros(6 * n)
+    lib.TDstressEachSourceAtReceiver_C(r[0], r[1], r[2], p(P1f), p(P2f), p(P3f), n, 0.0, 1.0, 0.0, mu, lam, True,
+                                       p(s), p(e))
+    out["hs_each_R"], out["hs_each_stress"], out["hs_each_strain"] = r, s.reshape(n, 6), e.reshape(n, 6)
+    return out
+
+
 OUTPUT_FIELDS = ("Tno", "Tt", "Tt1o", "Tt2o", "rake", "state", "slipv", "slipv1", "slipv2", "a", "b", "dc", "fric",
                  "slip", "slip1", "slip2", "slipvC")
 
@@ -284,7 +361,7 @@ def output_case(work, QDsim_mod):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", default=None, help="regenerate one fixture: gf | tiny | output")
+    ap.add_argument("--only", default=None, help="regenerate one fixture: gf | tiny | hs | output")
     args = ap.parse_args()
     ref_src = os.path.join(args.ref, "src")
     subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref", "REFSRC=" + os.path.join(ref_src, "TDstressFS_C.cpp")],
@@ -309,13 +386,16 @@ def main():
         if args.only in (None, "tiny"):
             t = tiny_case(work, QDsim, readmsh, Hmatrix)
             np.savez_compressed(os.path.join(HERE, "tiny_case.npz"), **t)
+        if args.only in (None, "hs"):
+            h = hs_cases(lib, SH_greenfunction)
+            np.savez_compressed(os.path.join(HERE, "hs_cases.npz"), **h)
         if args.only in (None, "output"):
             o = output_case(work, QDsim)
             np.savez_compressed(os.path.join(HERE, "output_case.npz"), **o)
     finally:
         os.chdir(cwd)
         shutil.rmtree(work, ignore_errors=True)
-    for f in ("gf_cases.npz", "tiny_case.npz", "output_case.npz"):
+    for f in ("gf_cases.npz", "tiny_case.npz", "hs_cases.npz", "output_case.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
 
 

@@ -1,8 +1,13 @@
-"""The C restatement of TDstressFS (oracle/td_oracle.c) against the reference's own
-outputs: its library built from source and its numpy twin (tests/golden/gf_cases.npz)."""
+"""The C restatement of TDstressFS / TDstressHS (oracle/td_oracle.c) against the
+reference's own outputs: its library built from source and its numpy twin
+(tests/golden/gf_cases.npz, tests/golden/hs_cases.npz)."""
+import os
+
 import numpy as np
+import pytest
 
 import qd_oracle
+from conftest import GOLDEN
 
 
 def _rel(a, b):
@@ -65,3 +70,54 @@ def test_special_points_cover_all_configurations(gf_golden):
     zero_rows = np.all(s == 0.0, axis=-1)
     assert zero_rows.any()          # casez: receivers on TD edge lines
     assert np.isfinite(s).any()
+
+
+# ---------------------------------------------------------------- half space
+HS_MODES = {"stress": 2, "numpy": 1}   # golden key suffix -> oracle mode (C++ path / numpy twin)
+
+
+@pytest.fixture(scope="module")
+def hs_golden():
+    return dict(np.load(os.path.join(GOLDEN, "hs_cases.npz")))
+
+
+@pytest.mark.parametrize("tag,b", [("ss", (1.0, 0.0, 0.0)), ("ds", (0.0, 1.0, 0.0)), ("mix", (0.7, -0.4, 0.25))])
+@pytest.mark.parametrize("src", ["stress", "numpy"])
+def test_oracle_halfspace_matches_reference(hs_golden, tag, b, src):
+    """The half-space restatement against the reference's C++ path (mode 2) and its
+    numpy twin (mode 1), on triangles at depth, touching the free surface, with a
+    side along z in each position, and vertical; receivers at depth, within 20 m
+    of the surface and on it.  1e-9 of each receiver's largest component."""
+    g = hs_golden
+    mu, lam = float(g["mu"]), float(g["lam"])
+    for t in range(len(g["hs_P"])):
+        R, P = g["hs_R"][t], g["hs_P"][t]
+        s, e = qd_oracle.td_stress_hs(R[:, 0], R[:, 1], R[:, 2], P[0], P[1], P[2], *b, mu, lam, HS_MODES[src])
+        ref = g["hs_%s_%s" % (tag, src)][t]
+        assert (np.abs(s - ref) <= 1e-9 * np.abs(ref).max(axis=1, keepdims=True)).all(), (t, g["hs_kind"][t])
+        if src == "stress":
+            refe = g["hs_%s_strain" % tag][t]
+            assert (np.abs(e - refe) <= 1e-9 * np.abs(refe).max(axis=1, keepdims=True)).all()
+
+
+def test_reference_paths_differ_only_for_later_vertical_sides(hs_golden):
+    """The reference's two half-space paths agree except when a side along z is not
+    the triangle's first side: the C++ path then repeats the previous side's term."""
+    g = hs_golden
+    for t, kind in enumerate(g["hs_kind"]):
+        d = np.abs(g["hs_ss_stress"][t] - g["hs_ss_numpy"][t]).max() / np.abs(g["hs_ss_numpy"][t]).max()
+        if kind in ("vertical_side2", "vertical_side3"):
+            assert d > 1e-3
+        else:
+            assert d < 1e-9, kind
+
+
+def test_oracle_halfspace_each_source(hs_golden):
+    g = hs_golden
+    mu, lam = float(g["mu"]), float(g["lam"])
+    r = g["hs_each_R"]
+    for t in range(len(g["hs_P"])):
+        P = g["hs_P"][t]
+        s, _ = qd_oracle.td_stress_hs([r[0]], [r[1]], [r[2]], P[0], P[1], P[2], 0.0, 1.0, 0.0, mu, lam, 2)
+        ref = g["hs_each_stress"][t]
+        assert np.abs(s[0] - ref).max() <= 1e-9 * np.abs(ref).max()
