@@ -42,8 +42,9 @@ extern "C" {
 /* Replaces TDstressFS_C (src/TDstressFS_C.cpp:2048-2095): stress and strain
  * (xx,yy,zz,xy,xz,yz per receiver, stress[i*6+c]) at n receivers (X,Y,Z) from one
  * triangular dislocation P1,P2,P3 with Burgers components (Ss strike, Ds dip,
- * Ts tensile).  Full space only: jud_halfspace=true is rejected (outputs NaN,
- * message on stderr). */
+ * Ts tensile).  jud_halfspace=true gives the half-space solution with the
+ * reference library's side handling (hs_mode 2 below), and prints the
+ * reference's warning when a z coordinate is positive. */
 void TDstressFS_C(const double *X, const double *Y, const double *Z, size_t n,
                   const double *P1, const double *P2, const double *P3,
                   double Ss, double Ds, double Ts, double mu, double lambda_,
@@ -69,14 +70,28 @@ size_t pq3d_src_record_bytes(void);
 int pq3d_src_records(const double *d_nodes, const int64_t *d_tri, int64_t n_elem,
                      void *d_rec, cudaStream_t stream);
 
+/* Half space (TDstressHS, src/TDstressFS_C.cpp:1911-2000): per-element records of
+ * the image triangle and the three sides' free-surface-correction frames.
+ * hs_mode of the entry points below: 0 full space (d_hs may be NULL); 1 half
+ * space, a triangle side along z adds no free-surface term (the reference's
+ * numpy TDstressHS, src/SH_greenfunction.py:734-888); 2 half space as the
+ * reference's compiled library, which lets such a side repeat the term of the
+ * side before it (src/TDstressFS_C.cpp:1517-1522) -- the values the reference's
+ * H-matrix assembly uses. */
+size_t pq3d_hs_record_bytes(void);
+int pq3d_hs_records(const double *d_nodes, const int64_t *d_tri, int64_t n_elem, void *d_hs,
+                    cudaStream_t stream);
+
 /* Tractions (A1s,A2s,Bs,A1d,A2d,Bd) for npairs (receiver, source) element pairs:
  * the entries BlockTree.calc_stressfunc_fromCS/CD compute (src/Hmatrix.py:425-511). */
 int pq3d_traction_pairs(const double *d_xg, const double *d_ev, const void *d_rec,
                         const int64_t *d_rows, const int64_t *d_cols, int64_t npairs,
-                        double mu, double lam, double *d_out, cudaStream_t stream);
+                        double mu, double lam, double *d_out, const void *d_hs, int hs_mode,
+                        cudaStream_t stream);
 
 /* Device form of both drop-ins: n_pts receivers x n_src sources, one of which is 1
- * (or both equal: pairwise).  d_P is n_src x 9 (P1,P2,P3). */
+ * (or both equal: pairwise).  d_P is n_src x 9 (P1,P2,P3).  halfspace: hs_mode
+ * (0, 1, 2 as above; the drop-ins use 2). */
 int pq3d_stress_points(const double *d_X, const double *d_Y, const double *d_Z, int64_t n_pts,
                        const double *d_P, int64_t n_src, double Ss, double Ds, double Ts,
                        double mu, double lam, int halfspace, double *d_stress,
@@ -90,7 +105,7 @@ int pq3d_stress_points(const double *d_X, const double *d_Y, const double *d_Z, 
 int pq3d_dense_assemble(const double *d_xg, const double *d_ev, const void *d_rec,
                         const int32_t *d_perm, const void *d_blocks, int64_t n_blocks,
                         double mu, double lam, double *d_out64, float *d_out32,
-                        cudaStream_t stream);
+                        const void *d_hs, int hs_mode, cudaStream_t stream);
 
 /* Workspace (doubles) of one ACA task with rank cap kmax. */
 int64_t pq3d_aca_ws_doubles(int m, int n, int kmax);
@@ -105,7 +120,7 @@ int pq3d_aca_batched(const double *d_xg, const double *d_ev, const void *d_rec,
                      const int32_t *d_rowlist, const int32_t *d_collist,
                      const void *d_tasks, int64_t n_tasks, double *d_ws, double mu,
                      double lam, double eps, int rel_mode, int max_mn, int32_t *d_rank,
-                     int32_t *d_flags, cudaStream_t stream);
+                     int32_t *d_flags, const void *d_hs, int hs_mode, cudaStream_t stream);
 
 /* Pack ACA factors into the matvec layout; dtype 0 FP64, 1 FP32, 2 BF16. */
 int pq3d_aca_pack(const void *d_tasks, int64_t n_tasks, const double *d_ws,

@@ -44,7 +44,7 @@ def td_lib():
             [ctypes.c_int, D, D]
         L.td_traction_block.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
                                                                  ctypes.c_double, ctypes.c_double, ctypes.c_int,
-                                                                 ctypes.c_void_p]
+                                                                 ctypes.c_int, ctypes.c_void_p]
         _td = L
     return _td
 
@@ -80,7 +80,10 @@ def td_stress_hs(X, Y, Z, P1, P2, P3, Ss, Ds, Ts, mu, lam, mode=2):
 
 
 class Geometry:
-    def __init__(self, xg, ev, nodes, tri, mu, lam):
+    """Elements of a mesh; hs_mode 0 full space, 1 / 2 half space (td_stress_hs)."""
+
+    def __init__(self, xg, ev, nodes, tri, mu, lam, hs_mode=0):
+        self.hs_mode = int(hs_mode)
         self.xg = np.ascontiguousarray(xg, dtype=np.float64)
         self.ev = np.ascontiguousarray(ev, dtype=np.float64)
         self.nodes = np.ascontiguousarray(nodes, dtype=np.float64)
@@ -96,7 +99,7 @@ class Geometry:
         out = np.zeros((3 * nm, m, n))
         td_lib().td_traction_block(self.xg.ctypes.data, self.ev.ctypes.data, self.nodes.ctypes.data,
                                    self.tri.ctypes.data, rows.ctypes.data, m, cols.ctypes.data, n, self.mu, self.lam,
-                                   which, out.ctypes.data)
+                                   which, self.hs_mode, out.ctypes.data)
         return out
 
 

@@ -248,13 +248,18 @@ static void td_traction(const double s[6], const double *ev, double t[3])
 
 /* Traction block: rows = receivers (centroids xg[ri], frames ev[ri]),
  * cols = source elements.  which: 1 strike slip (Ss=1), 2 dip slip (Ds=1),
- * 3 both.  out holds 3 planes per computed mode of m*n doubles, row-major, in
+ * 3 both; hs_mode 0 full space, 1 or 2 half space (td_stress_hs).  out holds
+ * 3 planes per computed mode of m*n doubles, row-major, in
  * the order A1, A2, B (strike first when both): the values of
  * calc_stressfunc_fromCS/CD and calc_stressfunc_fromC_rowS/D
  * (src/Hmatrix.py:318-511). */
+void td_stress_hs(const double obs[3], const double P1[3], const double P2[3], const double P3[3],
+                  double Ss, double Ds, double Ts, double mu, double lam, int mode,
+                  double stress[6], double strain[6]);
+
 void td_traction_block(const double *xg, const double *ev, const double *nodes, const long *tri,
                        const long *rows, size_t m, const long *cols, size_t n,
-                       double mu, double lam, int which, double *out)
+                       double mu, double lam, int which, int hs_mode, double *out)
 {
     int modes[2], nm = 0;
     if (which & 1) modes[nm++] = 0;
@@ -269,8 +274,12 @@ void td_traction_block(const double *xg, const double *ev, const double *nodes, 
             double s[6], t[3];
             for (int q = 0; q < nm; ++q) {
                 int slip = modes[q];
-                td_stress_fs(xg + 3 * r, P1, P2, P3, slip == 0 ? 1.0 : 0.0, slip == 0 ? 0.0 : 1.0, 0.0,
-                             mu, lam, s, 0);
+                if (hs_mode)
+                    td_stress_hs(xg + 3 * r, P1, P2, P3, slip == 0 ? 1.0 : 0.0, slip == 0 ? 0.0 : 1.0, 0.0,
+                                 mu, lam, hs_mode, s, 0);
+                else
+                    td_stress_fs(xg + 3 * r, P1, P2, P3, slip == 0 ? 1.0 : 0.0, slip == 0 ? 0.0 : 1.0, 0.0,
+                                 mu, lam, s, 0);
                 td_traction(s, ev + 9 * r, t);
                 for (int c = 0; c < 3; ++c) out[(size_t)(3 * q + c) * m * n + i * n + j] = t[c];
             }

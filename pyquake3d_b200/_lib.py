@@ -79,16 +79,18 @@ def load():
     L.TDstressEachSourceAtReceiver_C.restype = None
     L.pq3d_src_record_bytes.restype = ctypes.c_size_t
     L.pq3d_src_records.argtypes = [vp, vp, i64, vp, vp]
-    L.pq3d_traction_pairs.argtypes = [vp, vp, vp, vp, vp, i64, ctypes.c_double, ctypes.c_double, vp, vp]
+    L.pq3d_traction_pairs.argtypes = [vp, vp, vp, vp, vp, i64, ctypes.c_double, ctypes.c_double, vp, vp, i32, vp]
+    L.pq3d_hs_record_bytes.restype = ctypes.c_size_t
+    L.pq3d_hs_records.argtypes = [vp, vp, i64, vp, vp]
     L.pq3d_stress_points.argtypes = [vp, vp, vp, i64, vp, i64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_double, ctypes.c_double, i32, vp, vp, vp]
-    L.pq3d_dense_assemble.argtypes = [vp, vp, vp, vp, vp, i64, ctypes.c_double, ctypes.c_double, vp, vp, vp]
+    L.pq3d_dense_assemble.argtypes = [vp, vp, vp, vp, vp, i64, ctypes.c_double, ctypes.c_double, vp, vp, vp, i32, vp]
     L.pq3d_aca_ws_doubles.argtypes = [i32, i32, i32]
     L.pq3d_aca_ws_doubles.restype = i64
     L.pq3d_aca_task_bytes.restype = ctypes.c_size_t
     L.pq3d_pack_task_bytes.restype = ctypes.c_size_t
     L.pq3d_aca_batched.argtypes = [vp, vp, vp, vp, vp, vp, i64, vp, ctypes.c_double, ctypes.c_double,
-                                   ctypes.c_double, i32, i32, vp, vp, vp]
+                                   ctypes.c_double, i32, i32, vp, vp, vp, i32, vp]
     L.pq3d_aca_pack.argtypes = [vp, i64, vp, vp, vp, vp, i32, vp, vp, vp]
     L.pq3d_item_bytes.argtypes = [i32]
     L.pq3d_item_bytes.restype = ctypes.c_size_t
@@ -101,7 +103,7 @@ def load():
     L.pq3d_ens_args_bytes.restype = ctypes.c_size_t
     L.pq3d_ens_grid.argtypes = [i32]
     L.pq3d_ens_step.argtypes = [vp, i32, vp]
-    for f in ("pq3d_src_records", "pq3d_traction_pairs", "pq3d_stress_points", "pq3d_dense_assemble",
+    for f in ("pq3d_src_records", "pq3d_hs_records", "pq3d_traction_pairs", "pq3d_stress_points", "pq3d_dense_assemble",
               "pq3d_aca_batched", "pq3d_aca_pack", "pq3d_hmatvec", "pq3d_rk_grid", "pq3d_rk_step", "pq3d_ens_grid",
               "pq3d_ens_step", "pq3d_ens_task_rows", "pq3d_rk_rows_attempt", "pq3d_rk_rows_accept"):
         getattr(L, f).restype = ctypes.c_int

@@ -17,7 +17,8 @@ task), dense64 / dense32 (when assembled), U_<prec> / V_<prec> for each packed
 storage precision.
 
 The fingerprint is a SHA-256 over the element centroids and frames, the elastic
-constants, the cluster/admissibility/ACA parameters and the layout constants; a
+constants, the cluster/admissibility/ACA parameters, the half-space mode and
+the layout constants; a
 load with any of them different is refused (Pq3dError) rather than silently
 producing another operator.
 """
@@ -38,13 +39,14 @@ FILE_NAME = "operator.pq3d"
 _NP = {"float64": np.float64, "float32": np.float32, "int32": np.int32, "uint16": np.uint16, "uint8": np.uint8}
 
 
-def fingerprint(xg, ev, mu, lam, mini_leaf, eta, min_size, aca_tol, aca_rel, aca_seed, kcap, layout):
+def fingerprint(xg, ev, mu, lam, mini_leaf, eta, min_size, aca_tol, aca_rel, aca_seed, kcap, layout, halfspace=0):
     h = hashlib.sha256()
     h.update(np.ascontiguousarray(xg, dtype=np.float64).tobytes())
     h.update(np.ascontiguousarray(ev, dtype=np.float64).tobytes())
     h.update(json.dumps(dict(mu=float(mu), lam=float(lam), mini_leaf=int(mini_leaf), eta=float(eta),
                              min_size=int(min_size), aca_tol=float(aca_tol), aca_rel=bool(aca_rel),
-                             aca_seed=int(aca_seed), kcap=int(kcap), layout=layout), sort_keys=True).encode())
+                             aca_seed=int(aca_seed), kcap=int(kcap), layout=layout, halfspace=int(halfspace)),
+                        sort_keys=True).encode())
     return h.hexdigest()
 
 
@@ -57,7 +59,7 @@ def _layout(op):
 def op_fingerprint(op, xg, ev):
     s = op.s
     return fingerprint(xg, ev, op.mu, op.lam, s.mini_leaf, s.eta, s.min_size, op.aca_tol, op.aca_rel, op.aca_seed,
-                       op.kcap, _layout(op))
+                       op.kcap, _layout(op), getattr(op, "halfspace", 0))
 
 
 def _host(t):

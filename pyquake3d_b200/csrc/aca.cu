@@ -20,6 +20,7 @@
 #include <stdio.h>
 #include "pq3d_common.cuh"
 #include "td_gf.cuh"
+#include "td_hs.cuh"
 #include "hm_layout.cuh"
 #include <cuda_bf16.h>
 
@@ -119,6 +120,8 @@ __device__ inline bool bit_get(const uint32_t *bm, int i) { return (bm[i >> 5] >
 struct AcaCtx {
     const double *xg, *ev;
     const SrcRec *rec;
+    const HsRec *hs;      // half-space records (HS instantiation only)
+    int hs_mode;
     const int32_t *rows, *cols;
     double mu, lam, nu;
     int m, n, pass, k;
@@ -126,6 +129,7 @@ struct AcaCtx {
 };
 
 // Residual entries of rows I0..I0+cnt-1 (all columns): out[c][r][j] for comps < ncomp.
+template <bool HS>
 __device__ void residual_rows(const AcaCtx &C, int I0, int cnt, int ncomp, double *out, int ostride_c)
 {
     for (int r = 0; r < cnt; ++r) {
@@ -137,7 +141,9 @@ __device__ void residual_rows(const AcaCtx &C, int I0, int cnt, int ncomp, doubl
         for (int q = 0; q < 9; ++q) f[q] = C.ev[9 * re + q];
         for (int j = threadIdx.x; j < C.n; j += blockDim.x) {
             double t[3];
-            gf_traction_one(obs, f, C.rec[C.cols[j]], C.mu, C.lam, C.nu, C.pass, t);
+            if (HS) gf_traction_one_hs(obs, f, C.rec[C.cols[j]], C.hs[C.cols[j]], C.hs_mode, C.mu, C.lam, C.nu,
+                                       C.pass, t);
+            else gf_traction_one(obs, f, C.rec[C.cols[j]], C.mu, C.lam, C.nu, C.pass, t);
             for (int c = 0; c < ncomp; ++c) {
                 double v = t[c];
                 for (int q = 0; q < C.k; ++q)
@@ -149,6 +155,7 @@ __device__ void residual_rows(const AcaCtx &C, int I0, int cnt, int ncomp, doubl
 }
 
 // Residual entries of columns J0..J0+cnt-1 (all rows): out[c][r][i].
+template <bool HS>
 __device__ void residual_cols(const AcaCtx &C, int J0, int cnt, int ncomp, double *out, int ostride_c)
 {
     for (int r = 0; r < cnt; ++r) {
@@ -161,7 +168,8 @@ __device__ void residual_cols(const AcaCtx &C, int J0, int cnt, int ncomp, doubl
 #pragma unroll
             for (int q = 0; q < 9; ++q) f[q] = C.ev[9 * re + q];
             double t[3];
-            gf_traction_one(obs, f, s, C.mu, C.lam, C.nu, C.pass, t);
+            if (HS) gf_traction_one_hs(obs, f, s, C.hs[C.cols[J]], C.hs_mode, C.mu, C.lam, C.nu, C.pass, t);
+            else gf_traction_one(obs, f, s, C.mu, C.lam, C.nu, C.pass, t);
             for (int c = 0; c < ncomp; ++c) {
                 double v = t[c];
                 for (int q = 0; q < C.k; ++q)
@@ -185,11 +193,12 @@ __device__ ArgMax argmax_excl(int len, const uint32_t *bm, F f, ArgMax *red)
     return block_argmax(loc, red);
 }
 
+template <bool HS>
 __global__ void __launch_bounds__(ACA_THREADS)
 k_aca(const double *__restrict__ xg, const double *__restrict__ ev, const SrcRec *__restrict__ rec,
       const int32_t *__restrict__ rowlist, const int32_t *__restrict__ collist, const AcaTask *__restrict__ tasks,
       double *__restrict__ ws, double mu, double lam, double eps, int rel_mode, int32_t *__restrict__ rank_out,
-      int32_t *__restrict__ flag_out)
+      int32_t *__restrict__ flag_out, const HsRec *__restrict__ hs, int hs_mode)
 {
     extern __shared__ uint32_t bits[];
     __shared__ ArgMax red_am[32];
@@ -203,7 +212,7 @@ k_aca(const double *__restrict__ xg, const double *__restrict__ ev, const SrcRec
     for (int w = threadIdx.x; w < ((m + 31) >> 5) + ((n + 31) >> 5); w += blockDim.x) bits[w] = 0u;
 
     AcaCtx C;
-    C.xg = xg; C.ev = ev; C.rec = rec;
+    C.xg = xg; C.ev = ev; C.rec = rec; C.hs = hs; C.hs_mode = hs_mode;
     C.rows = rowlist + T.rows_off;
     C.cols = collist + T.cols_off;
     C.mu = mu; C.lam = lam; C.nu = 1.0 / (1.0 + lam / mu) / 2.0;
@@ -234,7 +243,7 @@ k_aca(const double *__restrict__ xg, const double *__restrict__ ev, const SrcRec
             if (attempt > max_attempts) { scan = 1; break; }
         }
         cnt = (Iref + 3 <= m) ? 3 : m - Iref;
-        residual_rows(C, Iref, cnt, 1, RIref, n);
+        residual_rows<HS>(C, Iref, cnt, 1, RIref, n);
         if (threadIdx.x == 0) s_scan = scan;
         __syncthreads();
         return Iref;
@@ -251,7 +260,7 @@ k_aca(const double *__restrict__ xg, const double *__restrict__ ev, const SrcRec
             if (attempt > max_attempts) { scan = 1; break; }
         }
         cnt = (Jref + 3 <= n) ? 3 : n - Jref;
-        residual_cols(C, Jref, cnt, 1, RJref, m);
+        residual_cols<HS>(C, Jref, cnt, 1, RJref, m);
         if (threadIdx.x == 0) s_scan = scan;
         __syncthreads();
         return Jref;
@@ -278,15 +287,15 @@ k_aca(const double *__restrict__ xg, const double *__restrict__ ev, const SrcRec
         int Istar = ic.i, Jstar = jc.i;
         if (Istar < 0 || Jstar < 0) { flags |= 4; break; }  // everything excluded
         if (ic.v > jc.v) {
-            residual_rows(C, Istar, 1, 3, RIs, n);
+            residual_rows<HS>(C, Istar, 1, 3, RIs, n);
             __syncthreads();
             Jstar = argmax_excl(n, prevJ, [&](int j) { return fabs(RIs[j]); }, red_am).i;
-            residual_cols(C, Jstar, 1, 3, RJs, m);
+            residual_cols<HS>(C, Jstar, 1, 3, RJs, m);
         } else {
-            residual_cols(C, Jstar, 1, 3, RJs, m);
+            residual_cols<HS>(C, Jstar, 1, 3, RJs, m);
             __syncthreads();
             Istar = argmax_excl(m, prevI, [&](int i) { return fabs(RJs[i]); }, red_am).i;
-            residual_rows(C, Istar, 1, 3, RIs, n);
+            residual_rows<HS>(C, Istar, 1, 3, RIs, n);
         }
         __syncthreads();
         const double alpha = RIs[Jstar], alpha1 = RIs[(int64_t)n + Jstar], alpha2 = RIs[2 * (int64_t)n + Jstar];
@@ -377,21 +386,29 @@ PQ3D_EXPORT int pq3d_aca_batched(const double *d_xg, const double *d_ev, const v
                                  const int32_t *d_rowlist, const int32_t *d_collist, const void *d_tasks,
                                  int64_t n_tasks, double *d_ws, double mu, double lam, double eps,
                                  int rel_mode, int max_mn, int32_t *d_rank, int32_t *d_flags,
-                                 cudaStream_t stream)
+                                 const void *d_hs, int hs_mode, cudaStream_t stream)
 {
     if (n_tasks < 0 || max_mn < 0) return PQ3D_ERR_ARG;
+    if (hs_mode < 0 || hs_mode > 2 || (hs_mode && !d_hs)) return PQ3D_ERR_ARG;
     if (n_tasks == 0) return PQ3D_OK;
     if (!d_xg || !d_ev || !d_rec || !d_rowlist || !d_collist || !d_tasks || !d_ws || !d_rank || !d_flags)
         return PQ3D_ERR_ARG;
     size_t smem = (size_t)(2 * ((max_mn + 31) / 32) + 2) * sizeof(uint32_t);
     if (smem > 200 * 1024) return PQ3D_ERR_ARG;
-    if (smem > 48 * 1024)
-        PQ3D_CHECK(cudaFuncSetAttribute(k_aca, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (smem > 48 * 1024) {
+        if (hs_mode) PQ3D_CHECK(cudaFuncSetAttribute(k_aca<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        else PQ3D_CHECK(cudaFuncSetAttribute(k_aca<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
     for (int64_t t0 = 0; t0 < n_tasks; t0 += 65535) {
         int64_t nt = n_tasks - t0 < 65535 ? n_tasks - t0 : 65535;
-        k_aca<<<(unsigned)nt, ACA_THREADS, smem, stream>>>(d_xg, d_ev, (const SrcRec *)d_rec, d_rowlist, d_collist,
-                                                          (const AcaTask *)d_tasks + t0, d_ws, mu, lam, eps,
-                                                          rel_mode, d_rank + t0, d_flags + t0);
+        if (hs_mode)
+            k_aca<true><<<(unsigned)nt, ACA_THREADS, smem, stream>>>(
+                d_xg, d_ev, (const SrcRec *)d_rec, d_rowlist, d_collist, (const AcaTask *)d_tasks + t0, d_ws, mu,
+                lam, eps, rel_mode, d_rank + t0, d_flags + t0, (const HsRec *)d_hs, hs_mode);
+        else
+            k_aca<false><<<(unsigned)nt, ACA_THREADS, smem, stream>>>(
+                d_xg, d_ev, (const SrcRec *)d_rec, d_rowlist, d_collist, (const AcaTask *)d_tasks + t0, d_ws, mu,
+                lam, eps, rel_mode, d_rank + t0, d_flags + t0, nullptr, 0);
     }
     return pq3d_launch_status();
 }

@@ -5,6 +5,7 @@
 #include <stdlib.h>
 #include "pq3d_common.cuh"
 #include "td_gf.cuh"
+#include "td_hs.cuh"
 #include "hm_layout.cuh"
 
 using namespace pq3d;
@@ -35,12 +36,36 @@ PQ3D_EXPORT int pq3d_src_records(const double *d_nodes, const int64_t *d_tri, in
     return pq3d_launch_status();
 }
 
+__global__ void k_hs_records(const double *__restrict__ nodes, const int64_t *__restrict__ tri, int64_t n_elem,
+                             HsRec *__restrict__ hs)
+{
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n_elem) return;
+    HsRec h;
+    make_hs_rec(nodes + 3 * (tri[3 * e + 0] - 1), nodes + 3 * (tri[3 * e + 1] - 1), nodes + 3 * (tri[3 * e + 2] - 1), h);
+    hs[e] = h;
+}
+
+PQ3D_EXPORT size_t pq3d_hs_record_bytes(void) { return sizeof(HsRec); }
+
+PQ3D_EXPORT int pq3d_hs_records(const double *d_nodes, const int64_t *d_tri, int64_t n_elem, void *d_hs,
+                                cudaStream_t stream)
+{
+    if (n_elem < 0 || (n_elem > 0 && (!d_nodes || !d_tri || !d_hs))) return PQ3D_ERR_ARG;
+    if (n_elem == 0) return PQ3D_OK;
+    k_hs_records<<<(unsigned)((n_elem + 127) / 128), 128, 0, stream>>>(d_nodes, d_tri, n_elem, (HsRec *)d_hs);
+    return pq3d_launch_status();
+}
+
+static bool hs_args_ok(const void *hs, int mode) { return mode == 0 || ((mode == 1 || mode == 2) && hs); }
+
 // ---------------------------------------------------------------- traction pairs
 // out[p*6 + 0..5] = (A1s, A2s, Bs, A1d, A2d, Bd) for receiver rows[p], source cols[p].
+template <bool HS>
 __global__ void k_traction_pairs(const double *__restrict__ xg, const double *__restrict__ ev,
                                  const SrcRec *__restrict__ rec, const int64_t *__restrict__ rows,
                                  const int64_t *__restrict__ cols, int64_t npairs, double mu, double lam,
-                                 double *__restrict__ out)
+                                 double *__restrict__ out, const HsRec *__restrict__ hs, int hs_mode)
 {
     int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (p >= npairs) return;
@@ -51,27 +76,35 @@ __global__ void k_traction_pairs(const double *__restrict__ xg, const double *__
 #pragma unroll
     for (int k = 0; k < 9; ++k) f[k] = ev[9 * r + k];
     double t[6];
-    gf_traction_sd(obs, f, rec[c], mu, lam, nu, t);
+    if (HS) gf_traction_sd_hs(obs, f, rec[c], hs[c], hs_mode, mu, lam, nu, t);
+    else gf_traction_sd(obs, f, rec[c], mu, lam, nu, t);
 #pragma unroll
     for (int k = 0; k < 6; ++k) out[6 * p + k] = t[k];
 }
 
 PQ3D_EXPORT int pq3d_traction_pairs(const double *d_xg, const double *d_ev, const void *d_rec,
                                     const int64_t *d_rows, const int64_t *d_cols, int64_t npairs,
-                                    double mu, double lam, double *d_out, cudaStream_t stream)
+                                    double mu, double lam, double *d_out, const void *d_hs, int hs_mode,
+                                    cudaStream_t stream)
 {
-    if (npairs < 0) return PQ3D_ERR_ARG;
+    if (npairs < 0 || !hs_args_ok(d_hs, hs_mode)) return PQ3D_ERR_ARG;
     if (npairs == 0) return PQ3D_OK;
     if (!d_xg || !d_ev || !d_rec || !d_rows || !d_cols || !d_out) return PQ3D_ERR_ARG;
     int th = 128;
-    k_traction_pairs<<<(unsigned)((npairs + th - 1) / th), th, 0, stream>>>(
-        d_xg, d_ev, (const SrcRec *)d_rec, d_rows, d_cols, npairs, mu, lam, d_out);
+    const unsigned g = (unsigned)((npairs + th - 1) / th);
+    if (hs_mode)
+        k_traction_pairs<true><<<g, th, 0, stream>>>(d_xg, d_ev, (const SrcRec *)d_rec, d_rows, d_cols, npairs, mu,
+                                                     lam, d_out, (const HsRec *)d_hs, hs_mode);
+    else
+        k_traction_pairs<false><<<g, th, 0, stream>>>(d_xg, d_ev, (const SrcRec *)d_rec, d_rows, d_cols, npairs, mu,
+                                                      lam, d_out, nullptr, 0);
     return pq3d_launch_status();
 }
 
 // ---------------------------------------------------------------- stress at points
 // Full stress/strain tensors for receivers (X,Y,Z) and sources rec[src[p]], general
 // Burgers vector (Ts, Ss, Ds); half-space adds the image and free-surface terms.
+template <bool HS>
 __global__ void k_stress_points(const double *__restrict__ X, const double *__restrict__ Y,
                                 const double *__restrict__ Z, int64_t xstride,
                                 const double *__restrict__ P, int64_t pstride, int64_t npairs,
@@ -93,6 +126,11 @@ __global__ void k_stress_points(const double *__restrict__ X, const double *__re
         const double b[1][3] = {{Ts, Ss, Ds}};
         double ee[1][6];
         td_strain_multi<1, true>(X1, s, nu, b, ee);
+        if (HS) {
+            HsRec h;
+            make_hs_rec(P1, P2, P3, h);
+            hs_add_strain<1, true>(obs, s, h, nu, b, halfspace, ee);
+        }
         for (int c = 0; c < 6; ++c) e[c] = ee[0][c];
         hooke(e, mu, lam, sig);
     }
@@ -115,11 +153,15 @@ PQ3D_EXPORT int pq3d_stress_points(const double *d_X, const double *d_Y, const d
     int64_t np = n_pts > n_src ? n_pts : n_src;
     if (n_pts == 0 || n_src == 0) return PQ3D_OK;
     if (!d_X || !d_Y || !d_Z || !d_P || !d_stress) return PQ3D_ERR_ARG;
-    if (halfspace) return PQ3D_ERR_ARG;  // half-space kernel not built into this library
+    if (halfspace < 0 || halfspace > 2) return PQ3D_ERR_ARG;
     int th = 128;
-    k_stress_points<<<(unsigned)((np + th - 1) / th), th, 0, stream>>>(
-        d_X, d_Y, d_Z, n_pts == 1 ? 0 : 1, d_P, n_src == 1 ? 0 : 1, np, Ss, Ds, Ts, mu, lam, halfspace,
-        d_stress, d_strain);
+    const unsigned g = (unsigned)((np + th - 1) / th);
+    if (halfspace)
+        k_stress_points<true><<<g, th, 0, stream>>>(d_X, d_Y, d_Z, n_pts == 1 ? 0 : 1, d_P, n_src == 1 ? 0 : 1, np,
+                                                    Ss, Ds, Ts, mu, lam, halfspace, d_stress, d_strain);
+    else
+        k_stress_points<false><<<g, th, 0, stream>>>(d_X, d_Y, d_Z, n_pts == 1 ? 0 : 1, d_P, n_src == 1 ? 0 : 1, np,
+                                                     Ss, Ds, Ts, mu, lam, 0, d_stress, d_strain);
     return pq3d_launch_status();
 }
 
@@ -150,7 +192,7 @@ static int stress_host(const double *X, const double *Y, const double *Z, size_t
         cudaMemcpy(dX + 2 * npt, Z, npt * sizeof(double), cudaMemcpyHostToDevice);
         cudaMemcpy(dP, P9, 9 * nsrc * sizeof(double), cudaMemcpyHostToDevice);
         rc = pq3d_stress_points(dX, dX + npt, dX + 2 * npt, (int64_t)npt, dP, (int64_t)nsrc, Ss, Ds, Ts, mu,
-                                lam, hs ? 1 : 0, dS, dS + 6 * np, 0);
+                                lam, hs ? 2 : 0, dS, dS + 6 * np, 0);
         if (rc == PQ3D_OK && cudaDeviceSynchronize() != cudaSuccess) rc = PQ3D_ERR_CUDA;
         if (rc == PQ3D_OK) {
             if (cudaMemcpy(stress, dS, 6 * np * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) rc = PQ3D_ERR_CUDA;
@@ -223,10 +265,12 @@ PQ3D_EXPORT void TDstressEachSourceAtReceiver_C(double x, double y, double z, co
 // One CTA per dense block (blocks listed largest first).  Entry (i, j) of block b is the
 // traction at the element in tree position r0+i due to the element in tree position c0+j,
 // written straight into the packed matvec layout (FP64 and/or FP32 copies).
+template <bool HS>
 __global__ void k_dense_assemble(const double *__restrict__ xg, const double *__restrict__ ev,
                                  const SrcRec *__restrict__ rec, const int32_t *__restrict__ perm,
                                  const DenseBlock *__restrict__ blocks, double mu, double lam,
-                                 double *__restrict__ out64, float *__restrict__ out32)
+                                 double *__restrict__ out64, float *__restrict__ out32,
+                                 const HsRec *__restrict__ hs, int hs_mode)
 {
     const DenseBlock B = blocks[blockIdx.x];
     const double nu = 1.0 / (1.0 + lam / mu) / 2.0;
@@ -239,7 +283,8 @@ __global__ void k_dense_assemble(const double *__restrict__ xg, const double *__
 #pragma unroll
         for (int k = 0; k < 9; ++k) f[k] = ev[9 * r + k];
         double t[6];
-        gf_traction_sd(obs, f, rec[c], mu, lam, nu, t);
+        if (HS) gf_traction_sd_hs(obs, f, rec[c], hs[c], hs_mode, mu, lam, nu, t);
+        else gf_traction_sd(obs, f, rec[c], mu, lam, nu, t);
 #pragma unroll
         for (int slip = 0; slip < 2; ++slip)
 #pragma unroll
@@ -254,16 +299,21 @@ __global__ void k_dense_assemble(const double *__restrict__ xg, const double *__
 PQ3D_EXPORT int pq3d_dense_assemble(const double *d_xg, const double *d_ev, const void *d_rec,
                                     const int32_t *d_perm, const void *d_blocks, int64_t n_blocks,
                                     double mu, double lam, double *d_out64, float *d_out32,
-                                    cudaStream_t stream)
+                                    const void *d_hs, int hs_mode, cudaStream_t stream)
 {
-    if (n_blocks < 0) return PQ3D_ERR_ARG;
+    if (n_blocks < 0 || !hs_args_ok(d_hs, hs_mode)) return PQ3D_ERR_ARG;
     if (n_blocks == 0) return PQ3D_OK;
     if (!d_xg || !d_ev || !d_rec || !d_perm || !d_blocks || (!d_out64 && !d_out32)) return PQ3D_ERR_ARG;
     for (int64_t b0 = 0; b0 < n_blocks; b0 += 65535) {
         int64_t nb = n_blocks - b0 < 65535 ? n_blocks - b0 : 65535;
-        k_dense_assemble<<<(unsigned)nb, 256, 0, stream>>>(d_xg, d_ev, (const SrcRec *)d_rec, d_perm,
-                                                          (const DenseBlock *)d_blocks + b0, mu, lam,
-                                                          d_out64, d_out32);
+        if (hs_mode)
+            k_dense_assemble<true><<<(unsigned)nb, 256, 0, stream>>>(d_xg, d_ev, (const SrcRec *)d_rec, d_perm,
+                                                                    (const DenseBlock *)d_blocks + b0, mu, lam,
+                                                                    d_out64, d_out32, (const HsRec *)d_hs, hs_mode);
+        else
+            k_dense_assemble<false><<<(unsigned)nb, 256, 0, stream>>>(d_xg, d_ev, (const SrcRec *)d_rec, d_perm,
+                                                                     (const DenseBlock *)d_blocks + b0, mu, lam,
+                                                                     d_out64, d_out32, nullptr, 0);
     }
     return pq3d_launch_status();
 }

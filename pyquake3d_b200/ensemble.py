@@ -109,12 +109,12 @@ class Ensemble:
         self.sims = list(sims)
         self.precision = precision
         s0 = self.sims[0]
+        from .qdsim import hs_mode
         for s in self.sims:
-            if s.halfspace_jud:
-                raise _lib.Pq3dError("half-space faults are not available in this build")
-            same = (s.mu, s.lambda_, s.V0, s.Cs, s.RelTol, bool(s.fix_Tn))
-            if same != (s0.mu, s0.lambda_, s0.V0, s0.Cs, s0.RelTol, bool(s0.fix_Tn)):
-                raise _lib.Pq3dError("ensemble faults must share elastic constants, V0, RelTol and Fix_Tn")
+            same = (s.mu, s.lambda_, s.V0, s.Cs, s.RelTol, bool(s.fix_Tn), hs_mode(s))
+            if same != (s0.mu, s0.lambda_, s0.V0, s0.Cs, s0.RelTol, bool(s0.fix_Tn), hs_mode(s0)):
+                raise _lib.Pq3dError("ensemble faults must share elastic constants, V0, RelTol, Fix_Tn and "
+                                     "the half-space setting")
         P = s0.Para0
         if share is not None:
             if len(share.sims) != len(self.sims):
@@ -132,7 +132,7 @@ class Ensemble:
             rel = P.get("ACA relative tolerance", "False") == "True"
             want = tuple(want or (("fp64",) if precision == "fp64" else ("fp64", precision)))
             self.op = DeviceHMatrix(self.struct, xg, ev, nodes, tri, s0.mu, s0.lambda_, device=device, aca_tol=tol,
-                                    aca_rel=rel).assemble(want)
+                                    aca_rel=rel, halfspace=hs_mode(s0)).assemble(want)
         self.n = n = self.struct.n
         self.M = M = self.struct.faults
         self.perm = self.struct.perm

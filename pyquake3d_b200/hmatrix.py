@@ -337,7 +337,10 @@ class DeviceHMatrix:
     U_ROWS = 512                                 # rows per U task (one CTA)
 
     def __init__(self, struct, xg, ev, nodes, tri, mu, lam, device="cuda", aca_tol=0.01, aca_rel=False,
-                 aca_seed=0, kcap=96, ws_budget_bytes=8 << 30, keep_factors=False):
+                 aca_seed=0, kcap=96, ws_budget_bytes=8 << 30, keep_factors=False, halfspace=0):
+        """halfspace: 0 full space; 1 half space, a triangle side along z adds no
+        free-surface term; 2 half space with the side handling of the reference's
+        compiled library (the values its H-matrix assembly uses)."""
         import torch
         self.torch = torch
         self.L = _lib.load()
@@ -361,6 +364,13 @@ class DeviceHMatrix:
         self._stream = _lib.stream_ptr()
         check(self.L.pq3d_src_records(ptr(self.nodes), ptr(self.tri), self.n, ptr(self.rec), self._stream),
               "pq3d_src_records")
+        self.halfspace = int(halfspace)
+        self.hs = None
+        if self.halfspace:
+            hb = self.L.pq3d_hs_record_bytes()
+            self.hs = torch.empty((self.n * hb + 7) // 8, **f64)
+            check(self.L.pq3d_hs_records(ptr(self.nodes), ptr(self.tri), self.n, ptr(self.hs), self._stream),
+                  "pq3d_hs_records")
         self.dense_blocks = [b for b in struct.blocks if not b.aca]
         self.aca_blocks = [b for b in struct.blocks if b.aca]
         self.plans = {}
@@ -406,7 +416,7 @@ class DeviceHMatrix:
             d_recs = torch.from_numpy(recs[order].view(np.uint8)).to(self.dev)
             check(self.L.pq3d_dense_assemble(ptr(self.xg), ptr(self.ev), ptr(self.rec), ptr(self.perm), ptr(d_recs),
                                              len(recs), self.mu, self.lam, ptr(self.dense64), ptr(self.dense32),
-                                             self._stream), "pq3d_dense_assemble")
+                                             ptr(self.hs), self.halfspace, self._stream), "pq3d_dense_assemble")
             torch.cuda.synchronize()
 
     def _run_aca(self):
@@ -471,7 +481,8 @@ class DeviceHMatrix:
                 check(self.L.pq3d_aca_batched(ptr(self.xg), ptr(self.ev), ptr(self.rec), ptr(self.rowlist),
                                               ptr(self.collist), ptr(d_rec), len(batch), ptr(ws), self.mu, self.lam,
                                               self.aca_tol, 1 if self.aca_rel else 0, max_mn, ptr(d_rank),
-                                              ptr(d_flag), self._stream), "pq3d_aca_batched")
+                                              ptr(d_flag), ptr(self.hs), self.halfspace, self._stream),
+                      "pq3d_aca_batched")
                 ranks = d_rank.cpu().numpy()
                 flags = d_flag.cpu().numpy()
                 keep = {}

@@ -299,9 +299,10 @@ class DeviceRowBackend:
         self.precision = precision
         P = sim.Para0
         if op is None:
+            from .qdsim import hs_mode
             op = DeviceHMatrix(self.rs, sim.xg, sim.eleVec, sim.nodelst, sim.elelst, sim.mu, sim.lambda_,
                                device=device, aca_tol=float(P.get("ACA tolerance", 0.01)),
-                               aca_rel=P.get("ACA relative tolerance", "False") == "True")
+                               aca_rel=P.get("ACA relative tolerance", "False") == "True", halfspace=hs_mode(sim))
             op.assemble(("fp64",) if precision == "fp64" else ("fp64", precision))
         self.op = op
         n = self.n = struct.n

@@ -17,6 +17,9 @@ behaviour by default):
   ACA seed                  seed of the ACA starting rows/cols (0)
   Precision                 fp64 | fp32 | bf16 operator storage (fp64)
   RK RelTol                 DP5(4) relative tolerance (1e-4)
+  Half space vertical sides reference | exact: free-surface term of a triangle
+                            side along z (the reference's compiled library
+                            repeats the previous side's term; exact adds none)
   Initial time step         htry (1e-3)
 """
 import math
@@ -39,6 +42,16 @@ def readPara0(fname):
                 tem = line.split(":")
                 para[tem[0].strip()] = tem[1].strip()
     return para
+
+
+def hs_mode(sim):
+    """Green's-function mode of a simulation: 0 full space; with `Half space: True`,
+    2 (the side handling of the reference's compiled library, which its H-matrix
+    assembly uses) unless `Half space vertical sides: exact` asks for 1 (a
+    triangle side along z adds no free-surface term)."""
+    if not sim.halfspace_jud:
+        return 0
+    return 1 if sim.Para0.get("Half space vertical sides", "reference").strip() == "exact" else 2
 
 
 def _flag(p, key, default=False):
@@ -333,14 +346,12 @@ class BlockTree:
 
     def _new_op(self):
         sim = self.sim
-        if sim.halfspace_jud:
-            raise _lib.Pq3dError("half-space Green's function is not available in this build")
         P = sim.Para0
         tol = float(P.get("ACA tolerance", 0.01))
         rel = P.get("ACA relative tolerance", "False") == "True"
         seed = int(P.get("ACA seed", 0))
         return DeviceHMatrix(self.struct, sim.xg, sim.eleVec, sim.nodelst, sim.elelst, sim.mu, sim.lambda_,
-                             device=sim.device, aca_tol=tol, aca_rel=rel, aca_seed=seed)
+                             device=sim.device, aca_tol=tol, aca_rel=rel, aca_seed=seed, halfspace=hs_mode(sim))
 
     def master(self, dir=None, blocks_to_process=None, num_workers=None, save_corefunc=False):
         """Assemble every block on the GPU (dense near field + batched ACA); with

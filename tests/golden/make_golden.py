@@ -27,6 +27,8 @@ What it does:
                         blocks use) for triangles at depth, touching the free
                         surface, with a vertical side and vertical; receivers at
                         depth, near and on the surface
+      tiny_hs_case.npz  the tiny case with `Half space: True` (its top edge lies on
+                        the free surface): operator products and 30 steps
       output_case.npz   seeded state fields on the tiny mesh and the SHA-256 of
                         the files QDsim.ouputVTK and QDsim.outputtxt write
                         for them (output formats, byte for byte)
@@ -358,10 +360,58 @@ def output_case(work, QDsim_mod):
     return out
 
 
+def tiny_hs_case(work, QDsim_mod, readmsh):
+    """The tiny fault (its top edge on the free surface) with `Half space: True`:
+    the reference's six operator products on fixed vectors and 30 simu_forward
+    steps (same seeded ACA starts as tiny_case)."""
+    t = np.load(os.path.join(HERE, "tiny_case.npz"))
+    d = os.path.join(work, "tiny_hs")
+    os.makedirs(d)
+    with open(os.path.join(d, "tiny.msh"), "w") as f:
+        f.write(str(t["msh"]))
+    with open(os.path.join(d, "tinyparam.dat"), "w") as f:
+        f.write(str(t["param_dat"]))
+    para_txt = str(t["parameter_txt"]).replace("Half space: False", "Half space: True")
+    assert "Half space: True" in para_txt
+    with open(os.path.join(d, "parameter.txt"), "w") as f:
+        f.write(para_txt)
+    nodes, tris = readmsh.read_mshV2(os.path.join(d, "tiny.msh"))
+    sim = QDsim_mod.QDsim(tris, nodes, os.path.join(d, "parameter.txt"))
+    assert sim.tree_block.halfspace_jud
+    tb = sim.tree_block
+    tb.blocks_to_process = []
+    tb.collect_blocks(tb.root_block)
+    blocks = tb.blocks_to_process
+    np.random.seed(int(t["aca_seed"]))
+    for b in blocks:
+        tb.ACA_worker(b)
+    out = {"parameter_txt": np.array(para_txt), "aca_seed": t["aca_seed"]}
+    ks = [b.ACA_dictS["U_ACA_A1s"].shape[1] for b in blocks if b.judaca]
+    kd = [b.ACA_dictD["U_ACA_A1d"].shape[1] for b in blocks if b.judaca]
+    out["aca_kS"], out["aca_kD"] = np.array(ks), np.array(kd)
+    X = t["mvm_x"]
+    out["mvm_x"] = X
+    for op in ("A1s", "A2s", "Bs", "A1d", "A2d", "Bd"):
+        x = X[0] if op.endswith("s") else X[1]
+        out["mvm_" + op] = tb.blocks_process_MVM(x, blocks, op)
+    sim.local_blocks = blocks
+    hs, ts = [], []
+    dttry = sim.htry
+    for i in range(30):
+        h, dtnext = sim.simu_forward(dttry)
+        hs.append(h)
+        ts.append(sim.time)
+        dttry = dtnext
+    out["steps_h"], out["steps_time"] = np.array(hs), np.array(ts)
+    for k in ("Tno", "Tt1o", "state", "slip1", "slip"):
+        out["step30_" + k] = np.array(getattr(sim, k), dtype=np.float64)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", default=None, help="regenerate one fixture: gf | tiny | hs | output")
+    ap.add_argument("--only", default=None, help="regenerate one fixture: gf | tiny | hs | tiny_hs | output")
     args = ap.parse_args()
     ref_src = os.path.join(args.ref, "src")
     subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref", "REFSRC=" + os.path.join(ref_src, "TDstressFS_C.cpp")],
@@ -389,13 +439,16 @@ def main():
         if args.only in (None, "hs"):
             h = hs_cases(lib, SH_greenfunction)
             np.savez_compressed(os.path.join(HERE, "hs_cases.npz"), **h)
+        if args.only in (None, "tiny_hs"):
+            th = tiny_hs_case(work, QDsim, readmsh)
+            np.savez_compressed(os.path.join(HERE, "tiny_hs_case.npz"), **th)
         if args.only in (None, "output"):
             o = output_case(work, QDsim)
             np.savez_compressed(os.path.join(HERE, "output_case.npz"), **o)
     finally:
         os.chdir(cwd)
         shutil.rmtree(work, ignore_errors=True)
-    for f in ("gf_cases.npz", "tiny_case.npz", "hs_cases.npz", "output_case.npz"):
+    for f in ("gf_cases.npz", "tiny_case.npz", "hs_cases.npz", "tiny_hs_case.npz", "output_case.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
 
 

@@ -100,7 +100,8 @@ def test_traction_pairs_all_pairs(lib, tiny_sim):
     _lib.check(lib.pq3d_src_records(nodes.data_ptr(), tri.data_ptr(), n, rec.data_ptr(), st), "records")
     out = torch.empty(n * n * 6, **f64)
     _lib.check(lib.pq3d_traction_pairs(xg.data_ptr(), ev.data_ptr(), rec.data_ptr(), op_rows.data_ptr(),
-                                       op_cols.data_ptr(), n * n, s.mu, s.lambda_, out.data_ptr(), st), "pairs")
+                                       op_cols.data_ptr(), n * n, s.mu, s.lambda_, out.data_ptr(), None, 0, st),
+               "pairs")
     got = out.cpu().numpy().reshape(n, n, 6).transpose(2, 0, 1)
     del dev
     scale = np.abs(ref).max(axis=(0, 2))[None, :, None]
