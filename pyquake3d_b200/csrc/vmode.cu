@@ -73,24 +73,24 @@ __device__ inline void mlp_features(double S, double lk, double a, double b, dou
     f[4] = (float)(log10(sig / 1e6) / 2.0);
 }
 
-// 5 -> 64 -> 64 -> 1 tanh network, FP32, parameters in shared memory.
-__device__ inline float mlp_eval(const float *P, const float *f)
+// 5 -> 64 -> 64 -> 1 tanh network, FP32 (parameters read through the read-only cache).
+__device__ inline float mlp_eval(const float *__restrict__ P, const float *f)
 {
     float h1[MLP_H];
 #pragma unroll 8
     for (int j = 0; j < MLP_H; ++j) {
-        float s = P[OFF_B1 + j];
+        float s = __ldg(P + OFF_B1 + j);
 #pragma unroll
-        for (int i = 0; i < 5; ++i) s += P[OFF_W1 + 5 * j + i] * f[i];
+        for (int i = 0; i < 5; ++i) s += __ldg(P + OFF_W1 + 5 * j + i) * f[i];
         h1[j] = tanhf(s);
     }
-    float out = P[OFF_B3];
+    float out = __ldg(P + OFF_B3);
 #pragma unroll 2
     for (int j = 0; j < MLP_H; ++j) {
-        float s = P[OFF_B2 + j];
+        float s = __ldg(P + OFF_B2 + j);
 #pragma unroll 16
-        for (int i = 0; i < MLP_H; ++i) s += P[OFF_W2 + MLP_H * j + i] * h1[i];
-        out += P[OFF_W3 + j] * tanhf(s);
+        for (int i = 0; i < MLP_H; ++i) s += __ldg(P + OFF_W2 + MLP_H * j + i) * h1[i];
+        out += __ldg(P + OFF_W3 + j) * tanhf(s);
     }
     return out;
 }
@@ -192,13 +192,12 @@ __device__ inline void write_x(const VArgs &A, int64_t i, double d1, double d2)
 
 __global__ void __launch_bounds__(VM_THREADS) k_vmode_stage(VArgs A, int s)
 {
-    __shared__ float P[MLP_NP];
     __shared__ double red[VM_THREADS / 32][2];
     __shared__ int s_last;
+    // MLP parameters are read in place through the read-only cache: only solves that
+    // fail the undamped-start test touch them, and a warp's lanes read the same weight.
     const bool use_mlp = A.seed_mode == 2 && A.mlp;
-    if (use_mlp)
-        for (int q = threadIdx.x; q < MLP_NP; q += VM_THREADS) P[q] = A.mlp[q];
-    __syncthreads();
+    const float *__restrict__ P = A.mlp;
     const int n = A.n;
     const double h = A.ctrl[0], t0 = A.ctrl[2];
     const double ts = t0 + kC[s - 1] * h;
