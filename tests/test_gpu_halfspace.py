@@ -8,13 +8,14 @@
 * half-space traction pairs on the tiny fault (top edge on the free surface)
   against the oracle's restatement;
 * QDsim with `Half space: True`: operator products and the 30-step dt sequence
-  of the reference's own run (tests/golden/tiny_hs_case.npz).
+  of the reference's own run (tests/golden/tiny_hs_case.npz), also with the
+  rows split over two emulated ranks; a half-space ensemble against its faults
+  run alone.
 Tolerances: Green's-function values 1e-9 of each receiver's largest component;
 operator products 1e-6 of their maximum (ACA+ magnifies ~1e-11 entry
 differences through small pivots; ranks are identical); steps 1e-8."""
 import ctypes
 import os
-import shutil
 
 import numpy as np
 import pytest
@@ -163,3 +164,47 @@ def test_halfspace_simulation_follows_reference(lib, tiny_hs_files):
     for k in ("Tno", "Tt1o", "state", "slip1", "slip"):
         ref = g["step30_" + k]
         assert np.abs(getattr(sim, k) - ref).max() <= 1e-7 * np.abs(ref).max(), k
+
+
+def test_halfspace_ensemble_follows_single_fault_runs(lib, tmp_path):
+    """Faults reaching the free surface, `Half space: True`, stepped together follow the
+    same faults run alone (FP64 operators)."""
+    from pyquake3d_b200 import QDsim, read_mshV2
+    from pyquake3d_b200.ensemble import Ensemble
+    from pyquake3d_b200.meshgen import ensemble_faults
+    files = ensemble_faults(str(tmp_path), n_faults=2, seed=7, lo=300, hi=700, edge=1.0)
+    for _, para in files:
+        txt = open(para).read().replace("Half space: False", "Half space: True")
+        open(para, "w").write(txt)
+
+    def sims():
+        out = []
+        for msh, para in files:
+            nodes, tris = read_mshV2(msh)
+            out.append(QDsim(tris, nodes, para, precision="fp64"))
+        return out
+    E = Ensemble(sims(), precision="fp64")
+    assert E.op.halfspace == 2
+    hist = E.run(15, [s.htry for s in E.sims])
+    for f, s in enumerate(sims()):
+        h1 = s._ensure_device().run(15, s.htry)
+        np.testing.assert_allclose(hist[:, f, 0], h1[:, 0], rtol=1e-9)
+
+
+def test_halfspace_two_ranks_follow_reference(lib, tiny_hs_files):
+    from pyquake3d_b200 import QDsim, read_mshV2
+    from pyquake3d_b200.partition import DeviceRowBackend, PartitionedStepper, TorchComm, row_partition
+    msh, para, g = tiny_hs_files
+    nodes, tris = read_mshV2(msh)
+    sim = QDsim(tris, nodes, para)
+    sim.Para0["ACA seed"] = str(int(g["aca_seed"]))
+    st = sim.tree_block.struct
+    b = row_partition(st, 2)
+    ps = PartitionedStepper([DeviceRowBackend(sim, st, b[r], b[r + 1], precision="fp64") for r in range(2)],
+                            TorchComm(use_dist=False), sim.RelTol)
+    dttry = sim.htry
+    hs = []
+    for _ in range(30):
+        h, dttry = ps.step(dttry)
+        hs.append(h)
+    np.testing.assert_allclose(hs, g["steps_h"], rtol=1e-8)

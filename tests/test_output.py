@@ -151,3 +151,14 @@ def test_checkpoint_rejects_foreign_files(tmp_path):
     p.write_bytes(checkpoint.MAGIC + struct.pack("<Q", len(hb)) + hb)
     with pytest.raises(_lib.Pq3dError):
         checkpoint.read_header(str(p))
+
+
+def test_checkpoint_fingerprint_covers_half_space():
+    from pyquake3d_b200 import checkpoint
+    op = _FakeOp()
+    xg, ev = np.zeros((40, 3)), np.zeros((40, 9))
+    fps = set()
+    for hs in (0, 1, 2):
+        op.halfspace = hs
+        fps.add(checkpoint.op_fingerprint(op, xg, ev))
+    assert len(fps) == 3
