@@ -48,6 +48,64 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def fp64_peak_tflops(n=8192, reps=3):
+    """Measured FP64 peak of this GPU: a cuBLAS DGEMM (n^3, FP64), CUDA-event timed."""
+    import torch
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        torch.matmul(a, b)
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / t / 1e12
+
+
+def gf_roofline(op, struct):
+    """Dense near-field assembly as a Green's-function roofline: (receiver, source)
+    pairs, pair-evaluations per second (strike and dip slip counted separately),
+    and, with the FP64 operations per pair counted by ncu on the same kernel
+    (profiles/gf_flops.json), the achieved FP64 rate against a measured DGEMM."""
+    import torch
+    pairs = int(struct.stats()["dense_entries"])
+    recs = op.dense_recs
+    from pyquake3d_b200._lib import check, ptr
+    order = np.argsort(-(recs["m"].astype(np.int64) * recs["n"]), kind="stable")
+    d_recs = torch.from_numpy(recs[order].view(np.uint8)).to(op.dev)
+    out32 = torch.empty_like(op.dense32) if op.dense32 is not None else None
+    out64 = None if out32 is not None else torch.empty_like(op.dense64)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def run():
+        check(op.L.pq3d_dense_assemble(ptr(op.xg), ptr(op.ev), ptr(op.rec), ptr(op.perm), ptr(d_recs), len(recs), op.mu,
+                                       op.lam, ptr(out64), ptr(out32), ptr(op.hs), op.halfspace, op._stream),
+              "pq3d_dense_assemble")
+    run()
+    torch.cuda.synchronize()
+    e0.record()
+    run()
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    del out32, out64
+    out = {"kernel": "k_dense_assemble (full space)", "pairs": pairs, "ms": 1e3 * t,
+           "pair_evals_per_s": 2 * pairs / t}
+    fp = os.path.join(REPO, "profiles", "gf_flops.json")
+    if os.path.exists(fp):
+        f = json.load(open(fp))
+        peak = fp64_peak_tflops()
+        ach = f["fp64_flops_per_pair"] * pairs / t / 1e12
+        out.update({"fp64_flops_per_pair": f["fp64_flops_per_pair"], "achieved_tflops": ach, "peak_tflops": peak,
+                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run", "frac": ach / peak})
+    return out
+
+
 def set_case(name):
     global CASE
     CASE = name
@@ -478,6 +536,9 @@ def main():
         mv[p] = {"ms": 1e3 * t, "GBs": plans[p]["alg_bytes"] / t / 1e9, "alg_bytes": int(plans[p]["alg_bytes"]),
                  "frac": plans[p]["alg_bytes"] / t / 1e9 / hbm, "stored_bytes": int(plans[p]["stored_bytes"])}
 
+    # Green's-function assembly roofline (FP64 compute bound)
+    gf = gf_roofline(op, sim.tree_block.struct)
+
     # accuracy vs the FP64 path at equal times (dt replay of the FP64 run), at several horizons
     accuracy = accuracy_study(sim, op, min(args.steps, 500), precisions=("bf16", "fp32"))
 
@@ -567,6 +628,7 @@ def main():
         "accuracy_vs_fp64": accuracy,
         "vmode": vmode,
         "ensemble": ensemble,
+        "gf_assembly": gf,
         "sim": {"time_s": float(hist[-1, 2]), "last_dt": float(hist[-1, 0]), "rejects": int(hist[:, 5].sum())},
         "e2e": e2e,
         "cpu_baseline": cpu,
