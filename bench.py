@@ -617,7 +617,7 @@ def main():
                    "assembly_s": round(t_asm, 2), "assembly_breakdown": {k: round(v, 3) for k, v in op.timings.items()}},
         "roofline": {"bound": "hbm", "achieved": mv[head]["GBs"], "peak": hbm, "unit": "GB/s",
                      "frac": mv[head]["frac"], "traffic": traffic,
-                     "kernel": "H-matvec (k_dense_v + k_u), " + prec_text[head].split(",")[0],
+                     "kernel": "H-matvec (k_v + k_du), " + prec_text[head].split(",")[0],
                      "alg_bytes": mv[head]["alg_bytes"], "ms": mv[head]["ms"], "peak_source": peak_kind},
         "slip_rel_err_vs_fp64": err_head.get("slip"),
         "plain_fp64": {"steps_per_s": rate["fp64"], "ms_per_step": 1e3 * timing["fp64"] / args.steps,

@@ -15,14 +15,20 @@
 // fixed order, so results are bitwise reproducible (no atomics).
 //
 // Launch sequence (stream-ordered, no host sync):
-//   k_dense_v   dense items and V items (t partials = V x per column chunk)
-//   k_u         per (low-rank block, row range): t from its chunk partials in
-//               shared memory, then slot rows = U_c t_c
+//   k_dense_v   V items (t partials = V x per column chunk); in FP64 also the
+//               dense items
+//   k_du        (FP32 / BF16) the dense items, then per (low-rank block, row
+//               range) a U task: t from its chunk partials in shared memory,
+//               slot rows = U_c t_c.  Launched with programmatic stream
+//               serialization, so its dense items run in k_dense_v's tail; the
+//               U tasks wait for k_dense_v.
+//   k_u         (FP64) the U tasks as a plain launch after k_dense_v.
 //   k_rowsum    y[i] = sum of row i's slots (FP64), plus optional loading terms
 //               (skipped when the step kernel sums the slots itself)
 #include "pq3d_common.cuh"
 #include "hm_layout.cuh"
 #include <cuda_bf16.h>
+#include <type_traits>
 
 using namespace pq3d;
 
@@ -82,18 +88,19 @@ template <>
 __device__ __forceinline__ double widen<double, double>(double v) { return v; }
 
 // ------------------------------------------------------------------ kernel 1
-// Dense items (lanes over block rows) and V items (up to 32 rows: 8 rows x 4
-// column groups per warp load, 4 rows per lane, then a 2-step shuffle reduction).
+// Work item of warp w: dense items (lanes over block rows) first, then V items (up
+// to 32 rows: 8 rows x 4 column groups per warp load, 4 rows per lane, then a
+// 2-step shuffle reduction) writing chunk partials of t = V x.
 template <typename TD, typename TL, typename TA>
-__global__ void __launch_bounds__(256)
-k_dense_v(const DenseItem *__restrict__ ditems, int64_t n_ditems, const VItem *__restrict__ vitems,
-          int64_t n_vitems, const TD *__restrict__ D, const TL *__restrict__ Vd, const TA *__restrict__ x,
-          int xstride, TA *__restrict__ slots, TA *__restrict__ tpart)
+__device__ __forceinline__ void dense_v_item(int64_t w, const DenseItem *__restrict__ ditems, int64_t n_ditems,
+                                             const VItem *__restrict__ vitems, int64_t n_vitems,
+                                             const TD *__restrict__ D, const TL *__restrict__ Vd,
+                                             const TA *__restrict__ x, int xstride, TA *__restrict__ slots,
+                                             TA *__restrict__ tpart)
 {
     constexpr int CWD = 16 / sizeof(TD);
     constexpr int CWV = 16 / sizeof(TL);
     const int lane = threadIdx.x & 31;
-    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (w < n_ditems) {
         const DenseItem it = ditems[w];
         const int r = it.r + lane;
@@ -163,6 +170,21 @@ k_dense_v(const DenseItem *__restrict__ ditems, int64_t n_ditems, const VItem *_
     }
 }
 
+// Kernel A: V items (and, in FP64, the dense items), one warp each.  Every CTA
+// lets the dependent kernel (k_du) launch as soon as it starts: k_du's dense
+// items do not read what this kernel writes and fill the SMs while its last wave
+// runs; k_du's U tasks wait for it.
+template <typename TD, typename TL, typename TA>
+__global__ void __launch_bounds__(256)
+k_dense_v(const DenseItem *__restrict__ ditems, int64_t n_ditems, const VItem *__restrict__ vitems,
+          int64_t n_vitems, const TD *__restrict__ D, const TL *__restrict__ Vd, const TA *__restrict__ x,
+          int xstride, TA *__restrict__ slots, TA *__restrict__ tpart)
+{
+    asm volatile("griddepcontrol.launch_dependents;");
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    dense_v_item<TD, TL, TA>(w, ditems, n_ditems, vitems, n_vitems, D, Vd, x, xstride, slots, tpart);
+}
+
 // ------------------------------------------------------------------ kernel 2
 // One CTA per (low-rank block, row range): sums the block's chunk partials of
 // t = V x into shared memory, then its warps stream U (lanes over rows).
@@ -191,6 +213,73 @@ __device__ __forceinline__ void smem_vec<double, 2>(const double *p, double *o)
     o[0] = a.x; o[1] = a.y;
 }
 
+template <typename TL, typename TA>
+__device__ __forceinline__ void u_task(const UTask &T, const TL *__restrict__ U, const TA *__restrict__ tpart,
+                                       TA *__restrict__ slots, TA *ts)
+{
+    constexpr int CW = 16 / sizeof(TL);
+    for (int e = threadIdx.x; e < 3 * T.K; e += blockDim.x) {
+        const int c = e / T.K, q = e % T.K;
+        int row = -1;
+        if (q < T.kS) row = c * T.kS + q;
+        else if (q < T.kS + T.kD) row = 3 * T.kS + c * T.kD + (q - T.kS);
+        TA v = 0;
+        if (row >= 0)
+            for (int ch = 0; ch < T.nch; ++ch) v += tpart[T.tp + (int64_t)ch * T.Q + row];
+        ts[e] = v;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ng = T.K / CW;
+    const int64_t gstride = (int64_t)T.m * 3 * CW;   // one column group of U: 3 comps x m rows
+    for (int rb = T.r0 + warp * 32; rb < T.r1; rb += blockDim.x) {
+        const int r = rb + lane;
+        if (r >= T.r1) break;
+        TA acc[3] = {0, 0, 0};
+        const TL *p = U + T.off + (int64_t)r * CW;             // [group][comp][row][CW]
+        const int64_t cstride = (int64_t)T.m * CW;
+#pragma unroll 2
+        for (int g = 0; g < ng; ++g) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                Vec16<TL> d = ld_stream(p + c * cstride);
+                TA tv[CW];
+                smem_vec<TA, CW>(ts + c * T.K + g * CW, tv);
+#pragma unroll
+                for (int k = 0; k < CW; ++k) acc[c] += widen<TA>(d.v[k]) * tv[k];
+            }
+            p += gstride;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) slots[3 * ((int64_t)T.slot + r) + c] = acc[c];
+    }
+}
+
+// Kernel B: CTAs [0, n_dblocks) run dense items (eight warps, one item each);
+// the remaining CTAs run one U task each.  Launched with programmatic stream
+// serialization after k_v: the dense CTAs start while k_v finishes, and a U
+// task waits (griddepcontrol.wait: k_v complete, its writes visible) before it
+// reads the chunk partials of t.
+template <typename TD, typename TL, typename TA>
+__global__ void __launch_bounds__(256)
+k_du(const DenseItem *__restrict__ ditems, int64_t n_ditems, int64_t n_dblocks, const UTask *__restrict__ tasks,
+     const TD *__restrict__ D, const TL *__restrict__ U, const TA *__restrict__ x, TA *__restrict__ slots,
+     const TA *__restrict__ tpart)
+{
+    if (blockIdx.x < n_dblocks) {
+        const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+        dense_v_item<TD, TL, TA>(w, ditems, n_ditems, nullptr, 0, D, nullptr, x, 0, slots, nullptr);
+        return;
+    }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const UTask T = tasks[blockIdx.x - n_dblocks];
+    u_task<TL, TA>(T, U, tpart, slots, reinterpret_cast<TA *>(smraw));
+}
+
+
+// FP64 path: the U tasks as their own launch after k_dense_v (dense and V items
+// together), which measured faster at this precision than the split launch.
 template <typename TL, typename TA>
 __global__ void __launch_bounds__(256)
 k_u(const UTask *__restrict__ tasks, const TL *__restrict__ U, const TA *__restrict__ tpart, TA *__restrict__ slots)
@@ -313,19 +402,49 @@ template <typename TD, typename TL, typename TA>
 static int run_matvec(const HmPlan &P, const TA *x, TA *slots, TA *tpart, const double *add0,
                       const double *add1, const double *add2, double *y, cudaStream_t st)
 {
-    const int64_t warps1 = P.n_ditems + P.n_vitems;
-    if (warps1 > 0) {
-        int64_t blocks = (warps1 * 32 + 255) / 256;
-        k_dense_v<TD, TL, TA><<<(unsigned)blocks, 256, 0, st>>>(
-            (const DenseItem *)P.ditems, P.n_ditems, (const VItem *)P.vitems, P.n_vitems, (const TD *)P.dense,
-            (const TL *)P.V, x, x_stride(P.n), slots, tpart);
+    // FP32 / BF16: V items first, dense items and U tasks in the dependent launch (the
+    // dense items fill the first launch's tail).  FP64: dense and V items together,
+    // then the U tasks (measured faster at this precision).
+    const bool split = !std::is_same<TD, double>::value;
+    const int64_t nd_a = split ? 0 : P.n_ditems, nd_b = split ? P.n_ditems : 0;
+    if (P.n_vitems + nd_a > 0) {
+        const int64_t blocks = ((P.n_vitems + nd_a) * 32 + 255) / 256;
+        k_dense_v<TD, TL, TA><<<(unsigned)blocks, 256, 0, st>>>((const DenseItem *)P.ditems, nd_a,
+                                                                (const VItem *)P.vitems, P.n_vitems,
+                                                                (const TD *)P.dense, (const TL *)P.V, x,
+                                                                x_stride(P.n), slots, tpart);
     }
-    if (P.n_utasks > 0) {
-        const size_t smem = (size_t)3 * P.kmax * sizeof(TA);
-        if (smem > 200 * 1024) return PQ3D_ERR_ARG;
-        if (smem > 48 * 1024)
-            PQ3D_CHECK(cudaFuncSetAttribute(k_u<TL, TA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_u<TL, TA><<<(unsigned)P.n_utasks, 256, smem, st>>>((const UTask *)P.utasks, (const TL *)P.U, tpart, slots);
+    if (!split) {
+        if (P.n_utasks > 0) {
+            const size_t smem = (size_t)3 * P.kmax * sizeof(TA);
+            if (smem > 200 * 1024) return PQ3D_ERR_ARG;
+            if (smem > 48 * 1024)
+                PQ3D_CHECK(cudaFuncSetAttribute(k_u<TL, TA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_u<TL, TA><<<(unsigned)P.n_utasks, 256, smem, st>>>((const UTask *)P.utasks, (const TL *)P.U, tpart,
+                                                                 slots);
+        }
+    } else {
+        const int64_t n_dblocks = (nd_b * 32 + 255) / 256;
+        const int64_t grid = n_dblocks + P.n_utasks;
+        if (grid > 0) {
+            const size_t smem = P.n_utasks > 0 ? (size_t)3 * P.kmax * sizeof(TA) : 0;
+            if (smem > 200 * 1024) return PQ3D_ERR_ARG;
+            if (smem > 48 * 1024)
+                PQ3D_CHECK(cudaFuncSetAttribute(k_du<TD, TL, TA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)grid);
+            cfg.blockDim = dim3(256);
+            cfg.dynamicSmemBytes = smem;
+            cfg.stream = st;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attr[0].val.programmaticStreamSerializationAllowed = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = (P.n_vitems + nd_a) > 0 ? 1 : 0;
+            PQ3D_CHECK(cudaLaunchKernelEx(&cfg, k_du<TD, TL, TA>, (const DenseItem *)P.ditems, nd_b, n_dblocks,
+                                          (const UTask *)P.utasks, (const TD *)P.dense, (const TL *)P.U, x, slots,
+                                          (const TA *)tpart));
+        }
     }
     if (y)
         k_rowsum<TA><<<(P.n + 255) / 256, 256, 0, st>>>(P.n, P.leaf_of_row, P.leaf_ptr, P.leaf_off, slots, add0,
