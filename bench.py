@@ -442,6 +442,15 @@ def main():
             dist.destroy_process_group()
         return
 
+    # batched ensemble of 32 independent faults (one launch per step for all); run first,
+    # on an empty device: its ACA workspaces (all live until packing) are the run's peak
+    ensemble = None
+    if not args.no_ensemble and world == 1:
+        ensemble = ensemble_study(args.ensemble_steps, 200)
+        import gc
+        gc.collect()
+        torch.cuda.empty_cache()
+
     from pyquake3d_b200 import QDsim, read_mshV2
     from pyquake3d_b200.qdsim import DeviceStepper
     msh, para = make_case(rank)
@@ -547,11 +556,6 @@ def main():
     vmode = None
     if not args.no_vmode:
         vmode = vmode_study(sim, op, args.vmode_steps)
-
-    # batched ensemble of 32 independent faults (one launch per step for all)
-    ensemble = None
-    if not args.no_ensemble and world == 1:
-        ensemble = ensemble_study(args.ensemble_steps, 200)
 
     # end to end through the reference call surface (QDsim.simu_forward) with the
     # reference main loop's per-step host traffic
