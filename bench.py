@@ -562,9 +562,7 @@ def main():
     mixed = steppers[head]
     sim._dev = mixed
     ne = min(args.steps, 300)
-    perm_t = torch.as_tensor(op.s.iperm, device=op.dev)
-    pin_v = torch.empty(sim.xg.shape[0], dtype=torch.float64).pin_memory()
-    pin_t = torch.empty_like(pin_v).pin_memory()
+    sim.snapshot_async(("slipv", "Tt"))           # allocates the pinned buffers once
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -572,14 +570,15 @@ def main():
     dttry = dts[head]
     for _ in range(ne):
         h, dttry = sim.simu_forward(dttry)
-        pin_v.copy_(mixed.t["slipv"].index_select(0, perm_t), non_blocking=True)
-        pin_t.copy_(mixed.t["Tt"].index_select(0, perm_t), non_blocking=True)
+        done, _ = sim.snapshot_async(("slipv", "Tt"))   # slip rate and traction of this step to the host
+    torch.cuda.current_stream().wait_event(done)         # the last copy is inside the timed region
     e1.record()
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
     e2e = {"value": ne * world / t_e2e, "unit": "steps/s", "h2d_bytes_per_step": 8,
            "d2h_bytes_per_step": int(16 * 8 + 2 * 8 * sim.xg.shape[0]), "steps": ne,
-           "path": "QDsim.simu_forward per step + slip-rate and traction vectors to pinned host memory"}
+           "path": "QDsim.simu_forward per step + slip-rate and traction vectors to pinned host memory "
+                   "(QDsim.snapshot_async: side-stream copy overlapping the next step)"}
 
     # CPU baseline: the reference's step on the same operator (rank 0, N=1)
     cpu = None

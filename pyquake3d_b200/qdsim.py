@@ -308,6 +308,11 @@ class QDsim:
         self.time = st.time
         return h, dtnext
 
+    def snapshot_async(self, names=("slipv", "Tt")):
+        """Asynchronous copy of device state vectors to pinned host memory (element order);
+        see DeviceStepper.snapshot_async."""
+        return self._ensure_device().snapshot_async(names)
+
     def sync_to_host(self):
         """Copy the device state back into the reference attribute names (element order)."""
         if self._dev is not None:
@@ -488,6 +493,7 @@ class DeviceStepper:
         self.hforce_cap = self.hforce.numel()
 
     def step(self, dttry):
+        """One step from the host (QDsim.simu_forward): returns (h, dtnext)."""
         self.ctrl[0] = float(dttry)
         self.launch(self.steps)
         c = self.ctrl.cpu().numpy()
@@ -530,6 +536,40 @@ class DeviceStepper:
         self.steps += nsteps
         self.time = float(c[2])
         return self.hist.view(-1, 6).cpu().numpy()[:nsteps]
+
+    def snapshot_async(self, names):
+        """Start copying state vectors (element order) to pinned host memory without
+        holding up the next step: the gather runs on the compute stream, the copy on a
+        side stream into one of two alternating buffers.  Returns (event, {name: host
+        tensor}); the arrays are valid once event.synchronize() returns, and stay valid
+        until the snapshot after next (the buffer is then reused)."""
+        torch = self.torch
+        names = tuple(names)
+        if getattr(self, "_snap", None) is None or self._snap["names"] != names:
+            n = self.n
+            self._snap = {"names": names, "k": 0, "stream": torch.cuda.Stream(device=self.op.dev),
+                          "iperm": torch.as_tensor(np.argsort(self.perm), device=self.op.dev),
+                          "dev": [torch.empty((len(names), n), dtype=torch.float64, device=self.op.dev)
+                                  for _ in range(2)],
+                          "host": [torch.empty((len(names), n), dtype=torch.float64).pin_memory() for _ in range(2)],
+                          "done": [None, None]}
+        S = self._snap
+        b = S["k"]
+        S["k"] ^= 1
+        cur = torch.cuda.current_stream(self.op.dev)
+        if S["done"][b] is not None:
+            cur.wait_event(S["done"][b])             # the buffer's previous copy has finished
+        for j, nm in enumerate(names):
+            torch.index_select(self.t[nm], 0, S["iperm"], out=S["dev"][b][j])
+        ready = torch.cuda.Event()
+        ready.record(cur)
+        with torch.cuda.stream(S["stream"]):
+            S["stream"].wait_event(ready)
+            S["host"][b].copy_(S["dev"][b], non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(S["stream"])
+        S["done"][b] = done
+        return done, {nm: S["host"][b][j] for j, nm in enumerate(names)}
 
     def get(self, name):
         v = self.t[name].cpu().numpy()

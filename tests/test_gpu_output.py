@@ -114,3 +114,24 @@ def test_driver_outputs_and_checkpoint_reload(lib, tiny_files, tiny_golden, tmp_
     assert loaded and len(blocks) == len(probe.tree_block.struct.blocks)
     run(msh, para, steps=30, quiet=True)
     assert _step_lines("state.txt") == steps
+
+
+def test_async_snapshots_match_state(lib, tiny_files):
+    """QDsim.snapshot_async: host copies taken on a side stream (alternating buffers)
+    equal the synchronous read-back of the same step, step after step."""
+    from pyquake3d_b200 import QDsim, read_mshV2
+    nodes, tris = read_mshV2(tiny_files[0])
+    sim = QDsim(tris, nodes, tiny_files[1])
+    dttry = sim.htry
+    pending = []
+    for i in range(6):
+        h, dttry = sim.simu_forward(dttry)
+        st = sim._ensure_device()
+        ref = {k: st.get(k) for k in ("slipv", "Tt")}
+        done, host = sim.snapshot_async(("slipv", "Tt"))
+        pending.append((done, host, ref))
+        if len(pending) == 2:               # a buffer stays valid until the snapshot after next
+            d0, h0, r0 = pending.pop(0)
+            d0.synchronize()
+            for k in ("slipv", "Tt"):
+                assert np.array_equal(h0[k].numpy(), r0[k]), (i, k)
