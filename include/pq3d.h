@@ -152,7 +152,8 @@ int pq3d_rk_grid(int n);
  * RungeKutte_solve_Dormand_Prince, src/QDsim.py:892-1134), cooperative launch.
  * Control block ctrl: [0] dttry in / dtnext out, [1] accepted h, [2] time,
  * [3] rejects this step, [4] status, [5] max|V1|, [6] max|V2|, [8] steps,
- * [9] total rejects, [10] total attempts. */
+ * [9] total rejects, [10] total attempts.  A positive args.h_in is the trial
+ * size instead of ctrl[0] (the host's dttry without a write to device memory). */
 int pq3d_rk_step(const void *args, int grid, cudaStream_t stream);
 
 /* Row-partitioned step (one fault over several GPUs, each rank owning tree-order
@@ -215,6 +216,31 @@ int pq3d_mlp_train_step(float *d_P, float *d_M, float *d_V, const float *d_X, in
  * is cleared on the stream before each launch), so calls that overlap on the
  * GPU race.  Allocates nothing. */
 int pq3d_rk_step_noalloc(const void *args, int grid, cudaStream_t stream);
+
+/* ------------------------------------------------------- host-visible results */
+
+/* The host side of QDsim.simu_forward and of the reference main loop's per-step
+ * output (src/QDsim.py:892-1134, src/main.py:161-184: dtnext, max |V1|, max |V2|,
+ * slip rate and traction after every step), without copy operations on the
+ * compute stream.  Pinned host memory mapped into the device address space:
+ * *host for the host, *dev for kernels. */
+int pq3d_host_map_alloc(size_t bytes, void **host, void **dev);
+int pq3d_host_map_free(void *host);
+/* Events without timing; query returns 1 when complete, 0 when not. */
+int pq3d_event_create(void **ev);
+int pq3d_event_destroy(void *ev);
+int pq3d_event_record(void *ev, cudaStream_t stream);
+int pq3d_event_sync(void *ev);
+int pq3d_event_query(void *ev);
+/* Gather nf <= 8 tree-order state vectors (fields: host array of device
+ * pointers, n doubles each) into mapped host memory out_dev (nf x n, element
+ * order: out[j][e] = fields[j][iperm[e]]).  Runs on `side` after `ready` (may be
+ * NULL), records `done` there, and makes `compute` wait for `done`, so a step
+ * enqueued later on `compute` cannot overwrite the vectors while they are read.
+ * With RkArgs.ctrl_host set (mapped memory, 16 doubles), pq3d_rk_step also
+ * stores ctrl[0..11) there and then ctrl_host[15] = step_index + 1. */
+int pq3d_snapshot(int nf, const double *const *fields, const int64_t *iperm, int64_t n, double *out_dev,
+                  void *ready, void *done, cudaStream_t compute, cudaStream_t side);
 
 #ifdef __cplusplus
 }

@@ -31,10 +31,12 @@ HM_PLAN = np.dtype([("n", "i4"), ("dtype", "i4")] + [(p, "u8") for p in _PLAN_PT
                    [("kmax", "i4"), ("pad", "i4")], align=True)
 _RK_PTRS = ["Tno", "Tt1o", "Tt2o", "psi", "slip1", "slip2", "slipv1", "slipv2", "slipv", "rake", "Tt", "fric", "slip",
             "a", "b", "dc", "f0", "shear_loading", "normal_loading", "vplc", "cr0", "sr0",
-            "y", "cand", "blk", "x", "ctrl", "hist", "hforce", "bar", "slots", "leaf_of_row", "leaf_ptr", "leaf_off"]
+            "y", "cand", "blk", "x", "ctrl", "hist", "hforce", "bar", "slots", "leaf_of_row", "leaf_ptr", "leaf_off",
+            "ctrl_host"]
 RK_ARGS = np.dtype([(p, "u8") for p in _RK_PTRS] +
                    [("n", "i4"), ("fix_tn", "i4"), ("x_fp32", "i4"), ("step_index", "i4"), ("fuse_rowsum", "i4"),
-                    ("slots_fp32", "i4"), ("V0", "f8"), ("eta", "f8"), ("reltol", "f8")], align=True)
+                    ("slots_fp32", "i4"), ("V0", "f8"), ("eta", "f8"), ("reltol", "f8"), ("h_in", "f8")],
+                   align=True)
 
 _ENS_PTRS = ["Tno", "Tt1o", "Tt2o", "psi", "slip1", "slip2", "slipv1", "slipv2", "slipv", "rake", "Tt", "fric", "slip",
              "a", "b", "dc", "f0", "shear_loading", "normal_loading", "vplc", "cr0", "sr0",
@@ -100,12 +102,21 @@ def load():
     L.pq3d_rk_step.argtypes = [vp, i32, vp]
     L.pq3d_rk_rows_attempt.argtypes = [vp, i32, i32, i32, ctypes.c_double, i32, vp, vp]
     L.pq3d_rk_rows_accept.argtypes = [vp, i32, i32, i32, ctypes.c_double, vp, vp]
+    L.pq3d_host_map_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(vp), ctypes.POINTER(vp)]
+    L.pq3d_host_map_free.argtypes = [vp]
+    L.pq3d_event_create.argtypes = [ctypes.POINTER(vp)]
+    for f in ("pq3d_event_destroy", "pq3d_event_sync", "pq3d_event_query"):
+        getattr(L, f).argtypes = [vp]
+    L.pq3d_event_record.argtypes = [vp, vp]
+    L.pq3d_snapshot.argtypes = [i32, vp, vp, i64, vp, vp, vp, vp, vp]
     L.pq3d_ens_args_bytes.restype = ctypes.c_size_t
     L.pq3d_ens_grid.argtypes = [i32]
     L.pq3d_ens_step.argtypes = [vp, i32, vp]
     for f in ("pq3d_src_records", "pq3d_hs_records", "pq3d_traction_pairs", "pq3d_stress_points", "pq3d_dense_assemble",
               "pq3d_aca_batched", "pq3d_aca_pack", "pq3d_hmatvec", "pq3d_rk_grid", "pq3d_rk_step", "pq3d_ens_grid",
-              "pq3d_ens_step", "pq3d_ens_task_rows", "pq3d_rk_rows_attempt", "pq3d_rk_rows_accept"):
+              "pq3d_ens_step", "pq3d_ens_task_rows", "pq3d_rk_rows_attempt", "pq3d_rk_rows_accept",
+              "pq3d_host_map_alloc", "pq3d_host_map_free", "pq3d_event_create", "pq3d_event_destroy",
+              "pq3d_event_record", "pq3d_event_sync", "pq3d_event_query", "pq3d_snapshot"):
         getattr(L, f).restype = ctypes.c_int
     sizes = {"DenseItem": (L.pq3d_item_bytes(0), DENSE_ITEM.itemsize), "VItem": (L.pq3d_item_bytes(1), V_ITEM.itemsize),
              "UTask": (L.pq3d_item_bytes(2), U_TASK.itemsize),
@@ -142,6 +153,9 @@ def ptr(t):
 
 
 def stream_ptr(stream=None):
+    """cudaStream_t of a torch stream, of the current stream (None), or a raw handle (int)."""
+    if isinstance(stream, int):
+        return stream
     import torch
     s = stream if stream is not None else torch.cuda.current_stream()
     return s.cuda_stream

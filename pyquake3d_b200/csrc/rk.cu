@@ -34,8 +34,11 @@ struct RkArgs {
     unsigned *bar;       // bar[0] arrivals, bar[1] generation, bar[2] end-of-step count (zeroed once)
     const void *slots;   // when fuse_rowsum: per-row partial sums of the H-matvec
     const int32_t *leaf_of_row, *leaf_ptr, *leaf_off;
+    double *ctrl_host;   // mapped host memory (may be null): ctrl[0..11) after the step, then
+                         // ctrl_host[15] = step_index + 1 once those are stored
     int n, fix_tn, x_fp32, step_index, fuse_rowsum, slots_fp32;
     double V0, eta, reltol;
+    double h_in;         // > 0: the step's trial size (instead of ctrl[0])
 };
 
 // Grid-wide NaN-propagating max of four values.  Every CTA reduces its own
@@ -135,7 +138,7 @@ __global__ void __launch_bounds__(RK_THREADS, PQ3D_RK_MINB) k_rk_step(RkArgs A)
         for (int64_t i = tid0; i < n; i += stride) fused_rowsum(A, i);
     }
     const bool forced = A.hforce != nullptr;
-    StepCtl c{forced ? A.hforce[A.step_index] : A.ctrl[0], 0.0, 0, 0, false};
+    StepCtl c{forced ? A.hforce[A.step_index] : (A.h_in > 0.0 ? A.h_in : A.ctrl[0]), 0.0, 0, 0, false};
     c.dtnext = c.h;
 
     while (true) {
@@ -225,6 +228,12 @@ __global__ void __launch_bounds__(RK_THREADS, PQ3D_RK_MINB) k_rk_step(RkArgs A)
             A.ctrl[1] = h;
             A.ctrl[3] = nrjct;
             if (A.ctrl[4] == 0.0) A.ctrl[4] = (double)PQ3D_ERR_DT;
+        }
+        if (A.ctrl_host) {
+            // the host's copy, sequence number last (a step that ended early leaves it stale)
+            for (int k = 0; k < 11; ++k) A.ctrl_host[k] = A.ctrl[k];
+            __threadfence_system();
+            A.ctrl_host[15] = (double)A.step_index + 1.0;
         }
     }
 }

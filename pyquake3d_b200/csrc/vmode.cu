@@ -61,7 +61,7 @@ __device__ const double kB4[7] = {5179.0 / 57600, 0.0, 7571.0 / 16695, 393.0 / 6
 constexpr int VM_THREADS = 128;
 constexpr int MLP_H = 64;
 // parameter layout: W1[64][5], b1[64], W2[64][64], b2[64], W3[64], b3[1]
-constexpr int OFF_W1 = 0, OFF_B1 = 320, OFF_W2 = 384, OFF_B2 = 4480, OFF_W3 = 4544, OFF_B3 = 4608, MLP_NP = 4609;
+constexpr int OFF_W1 = 0, OFF_B1 = 320, OFF_W2 = 384, OFF_B2 = 4480, OFF_W3 = 4544, OFF_B3 = 4608;
 
 // MLP features of one solve: (log1p S, log10 kappa, a, b, log10 sigma), scaled to O(1).
 __device__ inline void mlp_features(double S, double lk, double a, double b, double sig, float *f)

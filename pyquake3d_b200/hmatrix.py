@@ -608,6 +608,7 @@ class DeviceHMatrix:
         P = self.plan(dtype)
         if y is None and not slots_only:
             y = self.torch.empty((self.n, 3), dtype=self.torch.float64, device=self.dev)
+        P["slots_owner"] = None     # the slots now hold this call's products
         st = _lib.stream_ptr(stream)
         check(self.L.pq3d_hmatvec(P["host_plan"].ctypes.data, ptr(x), ptr(P["slots"]), ptr(P["tpart"]),
                                   ptr(add[0]), ptr(add[1]), ptr(add[2]), None if slots_only else ptr(y), st),

@@ -22,8 +22,10 @@ behaviour by default):
                             repeats the previous side's term; exact adds none)
   Initial time step         htry (1e-3)
 """
+import ctypes
 import math
 import os
+import weakref
 
 import numpy as np
 
@@ -400,6 +402,46 @@ class BlockTree:
         return y[{"A1": 0, "A2": 1, "B": 2}[type[:-1]]]
 
 
+def _release_host_io(L, hosts, events):
+    for h in hosts:
+        L.pq3d_host_map_free(h)
+    for e in events:
+        L.pq3d_event_destroy(e)
+
+
+class HostEvent:
+    """Completion of a snapshot (a CUDA event without timing)."""
+
+    def __init__(self, L, ev):
+        self._L = L
+        self._ev = ev
+
+    def synchronize(self):
+        check(self._L.pq3d_event_sync(self._ev), "pq3d_event_sync")
+
+    def query(self):
+        rc = self._L.pq3d_event_query(self._ev)
+        if rc < 0:
+            check(rc, "pq3d_event_query")
+        return rc == 1
+
+
+class _StepGraph:
+    """CUDA graph of consecutive steps.  A replay rewrites the operator's slots
+    and advances the state, so it invalidates pre-launched products and the
+    stepper's step event."""
+
+    def __init__(self, graph, plan, stepper):
+        self.graph = graph
+        self.plan = plan
+        self.stepper = stepper
+
+    def replay(self):
+        self.plan["slots_owner"] = None
+        self.stepper._state_event = False
+        self.graph.replay()
+
+
 class DeviceStepper:
     """Device-resident state (tree order) and the per-step launch sequence:
     H-matvec of the deficit -> cooperative DP5(4) step kernel."""
@@ -436,6 +478,10 @@ class DeviceStepper:
         self.hist_cap = 0
         self.hforce = None
         self.hforce_cap = 0
+        self._token = object()          # plan["slots_owner"]: whose products the slots hold
+        self._io = None                 # mapped control block and step event (step())
+        self._state_event = False       # step_done marks the current state (no launch since)
+        self._snap = None
         self.x = op.new_x(precision)
         from .hmatrix import pack_x
         x0 = pack_x((sim.slipv1 - sim.slipvC * np.cos(sim.rake0))[self.perm],
@@ -473,9 +519,17 @@ class DeviceStepper:
 
     def launch(self, step_index=0, stream=None):
         """Enqueue one step (matvec + DP5(4) kernel) without host synchronization; the
-        step kernel reduces the matvec's per-row slots itself."""
+        step kernel reduces the matvec's per-row slots itself.  The trial size is the
+        device-carried ctrl[0]."""
         self.op.matvec(self.x, self.precision, stream=stream, slots_only=True)
+        self._rk(step_index, 0.0, stream)
+
+    def _rk(self, step_index, h_in, stream=None, ctrl_host=0):
+        """Enqueue the step kernel alone (the slots must hold the products of x)."""
+        self._state_event = False
         self.args["step_index"] = step_index
+        self.args["h_in"] = h_in
+        self.args["ctrl_host"] = ctrl_host
         # per-step records only while the buffers have room for this step index
         self.args["hist"] = self.hist.data_ptr() if self.hist is not None and step_index < self.hist_cap else 0
         if self.hforce is not None and step_index >= self.hforce_cap:
@@ -493,15 +547,55 @@ class DeviceStepper:
         self.hforce_cap = self.hforce.numel()
 
     def step(self, dttry):
-        """One step from the host (QDsim.simu_forward): returns (h, dtnext)."""
-        self.ctrl[0] = float(dttry)
-        self.launch(self.steps)
-        c = self.ctrl.cpu().numpy()
+        """One step from the host (QDsim.simu_forward): returns (h, dtnext).
+
+        The H-matvec needs only the deficit x, not the step size, so the products of
+        the NEXT step are enqueued before the host waits for this step's result: the
+        device works on them while the caller runs its own code between steps, and
+        the next call enqueues only the step kernel (dttry goes to it as a kernel
+        argument).  The step kernel stores its control block in mapped host memory,
+        so the host waits on an event and reads it without a copy.  The operator's
+        slots are shared by every stepper of this precision: any other matvec into
+        them, or a graph replay, clears the plan's slots_owner, and the products are
+        then computed again here."""
+        io = self._io if self._io is not None else self._host_io()
+        L = self.L
+        P = self.op.plan(self.precision)
+        stream = _lib.stream_ptr()
+        if P.get("slots_owner") is not self._token:
+            self.op.matvec(self.x, self.precision, slots_only=True)
+        self._rk(self.steps, float(dttry), stream, ctrl_host=io["ctrl_dev"])
+        check(L.pq3d_event_record(io["step_done"], stream), "pq3d_event_record")
+        self._state_event = True                      # step_done marks the state of this step
+        self.op.matvec(self.x, self.precision, slots_only=True)   # products for the next step
+        P["slots_owner"] = self._token
+        check(L.pq3d_event_sync(io["step_done"]), "pq3d_event_sync")
+        c = io["ctrl"]
+        if c[15] != self.steps + 1:
+            c = self.ctrl.cpu().numpy()                # the step ended early: the device copy has the status
+            if c[4] == 0:
+                raise _lib.Pq3dError("time step ended without storing its result")
         if c[4] != 0:
             raise _lib.Pq3dError(f"time step failed: status {int(c[4])} (h={c[1]:.3e}, rejects={int(c[3])})")
         self.steps += 1
         self.time = float(c[2])
         return float(c[1]), float(c[0])
+
+    def _host_io(self):
+        """Mapped host memory for the control block (16 doubles) and the step event,
+        created on first use and released with the stepper."""
+        L = self.L
+        h, d, ev = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        check(L.pq3d_host_map_alloc(16 * 8, ctypes.byref(h), ctypes.byref(d)), "pq3d_host_map_alloc")
+        rc = L.pq3d_event_create(ctypes.byref(ev))
+        if rc != 0:
+            L.pq3d_host_map_free(h)
+            check(rc, "pq3d_event_create")
+        ctrl = np.ctypeslib.as_array((ctypes.c_double * 16).from_address(h.value))
+        ctrl[:] = 0.0
+        self._io = {"ctrl": ctrl, "ctrl_dev": d.value, "step_done": ev.value}
+        weakref.finalize(self, _release_host_io, L, [h.value], [ev.value])
+        return self._io
 
     def capture(self, nsteps):
         """CUDA graph of nsteps consecutive steps (matvec + step kernel each).  The
@@ -522,7 +616,7 @@ class DeviceStepper:
             torch.cuda.synchronize()
             return None
         torch.cuda.current_stream().wait_stream(s)
-        return g
+        return _StepGraph(g, self.op.plan(self.precision), self)
 
     def run(self, nsteps, dttry):
         """nsteps steps back to back on the device; returns the history (nsteps x 6)."""
@@ -538,38 +632,53 @@ class DeviceStepper:
         return self.hist.view(-1, 6).cpu().numpy()[:nsteps]
 
     def snapshot_async(self, names):
-        """Start copying state vectors (element order) to pinned host memory without
-        holding up the next step: the gather runs on the compute stream, the copy on a
-        side stream into one of two alternating buffers.  Returns (event, {name: host
-        tensor}); the arrays are valid once event.synchronize() returns, and stay valid
-        until the snapshot after next (the buffer is then reused)."""
+        """Start copying state vectors (element order) to host memory without holding
+        up the next step.  One gather kernel on a side stream writes them straight
+        into mapped host memory, after the step that produced them (the step event
+        when no launch came since) and concurrently with the pre-launched H-matvec;
+        the next step kernel waits for it.  Two buffers alternate.  Returns (event,
+        {name: float64 array}); the arrays are valid once event.synchronize() returns
+        and stay valid until the snapshot after next (the buffer is then reused)."""
         torch = self.torch
+        L = self.L
         names = tuple(names)
-        if getattr(self, "_snap", None) is None or self._snap["names"] != names:
-            n = self.n
-            self._snap = {"names": names, "k": 0, "stream": torch.cuda.Stream(device=self.op.dev),
-                          "iperm": torch.as_tensor(np.argsort(self.perm), device=self.op.dev),
-                          "dev": [torch.empty((len(names), n), dtype=torch.float64, device=self.op.dev)
-                                  for _ in range(2)],
-                          "host": [torch.empty((len(names), n), dtype=torch.float64).pin_memory() for _ in range(2)],
-                          "done": [None, None]}
         S = self._snap
+        if S is None or S["names"] != names:
+            n, nf = self.n, len(names)
+            hosts, views, devs, events = [], [], [], []
+            for _ in range(2):
+                h, d, ev = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+                check(L.pq3d_host_map_alloc(nf * n * 8, ctypes.byref(h), ctypes.byref(d)), "pq3d_host_map_alloc")
+                hosts.append(h.value)
+                devs.append(d.value)
+                check(L.pq3d_event_create(ctypes.byref(ev)), "pq3d_event_create")
+                events.append(ev.value)
+                a = np.ctypeslib.as_array((ctypes.c_double * (nf * n)).from_address(h.value)).reshape(nf, n)
+                views.append({nm: a[j] for j, nm in enumerate(names)})
+            S = {"names": names, "k": 0, "side": torch.cuda.Stream(device=self.op.dev),
+                 "iperm": torch.as_tensor(np.argsort(self.perm), dtype=torch.int64, device=self.op.dev),
+                 "fields": np.array([self.t[nm].data_ptr() for nm in names], dtype=np.uint64),
+                 "dev": devs, "views": views, "done": [HostEvent(L, e) for e in events]}
+            if self._snap is not None:
+                self._snap["release"]()
+            S["release"] = weakref.finalize(self, _release_host_io, L, hosts, events)
+            self._snap = S
         b = S["k"]
         S["k"] ^= 1
-        cur = torch.cuda.current_stream(self.op.dev)
-        if S["done"][b] is not None:
-            cur.wait_event(S["done"][b])             # the buffer's previous copy has finished
-        for j, nm in enumerate(names):
-            torch.index_select(self.t[nm], 0, S["iperm"], out=S["dev"][b][j])
-        ready = torch.cuda.Event()
-        ready.record(cur)
-        with torch.cuda.stream(S["stream"]):
-            S["stream"].wait_event(ready)
-            S["host"][b].copy_(S["dev"][b], non_blocking=True)
-            done = torch.cuda.Event()
-            done.record(S["stream"])
-        S["done"][b] = done
-        return done, {nm: S["host"][b][j] for j, nm in enumerate(names)}
+        compute = _lib.stream_ptr()
+        ready = None
+        if self._io is not None and self._state_event:
+            ready = self._io["step_done"]
+        else:
+            # the state is whatever the compute stream has enqueued so far
+            io = self._io if self._io is not None else self._host_io()
+            check(L.pq3d_event_record(io["step_done"], compute), "pq3d_event_record")
+            self._state_event = True
+            ready = io["step_done"]
+        done = S["done"][b]
+        check(L.pq3d_snapshot(len(names), S["fields"].ctypes.data, S["iperm"].data_ptr(), self.n, S["dev"][b],
+                              ready, done._ev, compute, S["side"].cuda_stream), "pq3d_snapshot")
+        return done, S["views"][b]
 
     def get(self, name):
         v = self.t[name].cpu().numpy()
