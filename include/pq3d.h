@@ -233,14 +233,17 @@ int pq3d_event_record(void *ev, cudaStream_t stream);
 int pq3d_event_sync(void *ev);
 int pq3d_event_query(void *ev);
 /* Gather nf <= 8 tree-order state vectors (fields: host array of device
- * pointers, n doubles each) into mapped host memory out_dev (nf x n, element
- * order: out[j][e] = fields[j][iperm[e]]).  Runs on `side` after `ready` (may be
- * NULL), records `done` there, and makes `compute` wait for `done`, so a step
- * enqueued later on `compute` cannot overwrite the vectors while they are read.
- * With RkArgs.ctrl_host set (mapped memory, 16 doubles), pq3d_rk_step also
- * stores ctrl[0..11) there and then ctrl_host[15] = step_index + 1. */
-int pq3d_snapshot(int nf, const double *const *fields, const int64_t *iperm, int64_t n, double *out_dev,
-                  void *ready, void *done, cudaStream_t compute, cudaStream_t side);
+ * pointers, n doubles each) into host memory host_out (nf x n, element order:
+ * host_out[j][e] = fields[j][iperm[e]]) through the device staging buffer
+ * d_stage (nf x n).  On `side`, after `ready` (may be NULL): gather, record
+ * `gathered` (and make `compute` wait for it, so a step enqueued later on
+ * `compute` cannot overwrite the vectors before they are read), copy to
+ * host_out, record `done`.  With RkArgs.ctrl_host set (mapped memory, 16
+ * doubles), pq3d_rk_step also stores ctrl[0..11) there and then
+ * ctrl_host[15] = step_index + 1. */
+int pq3d_snapshot(int nf, const double *const *fields, const int64_t *iperm, int64_t n, double *d_stage,
+                  double *host_out, void *ready, void *gathered, void *done, cudaStream_t compute,
+                  cudaStream_t side);
 
 #ifdef __cplusplus
 }

@@ -108,7 +108,7 @@ def load():
     for f in ("pq3d_event_destroy", "pq3d_event_sync", "pq3d_event_query"):
         getattr(L, f).argtypes = [vp]
     L.pq3d_event_record.argtypes = [vp, vp]
-    L.pq3d_snapshot.argtypes = [i32, vp, vp, i64, vp, vp, vp, vp, vp]
+    L.pq3d_snapshot.argtypes = [i32, vp, vp, i64, vp, vp, vp, vp, vp, vp, vp]
     L.pq3d_ens_args_bytes.restype = ctypes.c_size_t
     L.pq3d_ens_grid.argtypes = [i32]
     L.pq3d_ens_step.argtypes = [vp, i32, vp]

@@ -4,12 +4,13 @@
 // every step (src/main.py:161-184).
 //
 // The host waits for one small control block per step and, for output, reads
-// state vectors in element order.  Both go through pinned host memory mapped
-// into the device address space: the step kernel's last CTA stores the control
-// block there itself, and the snapshot kernel gathers state vectors from tree
-// order straight into a host buffer on a side stream.  No copy operation enters
-// the compute stream; the only ordering is an event the compute stream waits on
-// before the next step kernel overwrites the state being read.
+// state vectors in element order.  The step kernel's last CTA stores the control
+// block in pinned host memory mapped into the device address space, so no copy
+// operation enters the compute stream.  Snapshots are gathered from tree order
+// on a side stream (high priority, so the gather runs between the waves of the
+// H-matvec enqueued before it) and moved to the host by the copy engine; the
+// compute stream waits only for the gather, before the next step kernel
+// overwrites the state being read.
 #include "pq3d_common.cuh"
 
 namespace {
@@ -21,8 +22,8 @@ struct SnapFields {
     const double *f[SNAP_MAX_FIELDS];
 };
 
-// out[j * n + e] = field_j[iperm[e]]: element order from tree order, written to
-// mapped host memory (consecutive threads write consecutive elements).
+// out[j * n + e] = field_j[iperm[e]]: element order from tree order
+// (consecutive threads write consecutive elements).
 __global__ void __launch_bounds__(SNAP_THREADS) k_snapshot(SnapFields F, int nf, const int64_t *__restrict__ iperm,
                                                            int64_t n, double *__restrict__ out)
 {
@@ -105,16 +106,21 @@ PQ3D_EXPORT int pq3d_event_query(void *ev)
     return PQ3D_ERR_CUDA;
 }
 
-// Snapshot of nf device state vectors (tree order, n doubles each) into the
-// mapped host buffer out_dev (nf x n, element order: out[j][e] = field_j[iperm[e]]).
-// The gather runs on `side` after `ready` (recorded by the caller after the step
-// that produced the state); `done` is recorded on `side` after it, and `compute`
-// waits for `done`, so the next step kernel on `compute` cannot overwrite the
-// state while it is read.  The host buffer is complete once `done` has completed.
-PQ3D_EXPORT int pq3d_snapshot(int nf, const double *const *fields, const int64_t *iperm, int64_t n, double *out_dev,
-                              void *ready, void *done, cudaStream_t compute, cudaStream_t side)
+// Snapshot of nf device state vectors (tree order, n doubles each) into host
+// memory (nf x n, element order: host_out[j][e] = field_j[iperm[e]]).  On `side`,
+// after `ready` (recorded by the caller after the step that produced the state):
+// the gather kernel writes the device staging buffer d_stage (nf x n), `gathered`
+// is recorded and `compute` waits for it, so the next step kernel on `compute`
+// cannot overwrite the state before it is read, but does not wait for the
+// transfer; the copy engine then moves d_stage to host_out and `done` is
+// recorded.  host_out is complete once `done` has completed.  d_stage and
+// host_out must not be reused before `done`.
+PQ3D_EXPORT int pq3d_snapshot(int nf, const double *const *fields, const int64_t *iperm, int64_t n, double *d_stage,
+                              double *host_out, void *ready, void *gathered, void *done, cudaStream_t compute,
+                              cudaStream_t side)
 {
-    if (nf <= 0 || nf > SNAP_MAX_FIELDS || !fields || !iperm || n <= 0 || !out_dev || !done) return PQ3D_ERR_ARG;
+    if (nf <= 0 || nf > SNAP_MAX_FIELDS || !fields || !iperm || n <= 0 || !d_stage || !host_out || !gathered || !done)
+        return PQ3D_ERR_ARG;
     SnapFields F = {};
     for (int j = 0; j < nf; ++j) {
         if (!fields[j]) return PQ3D_ERR_ARG;
@@ -125,10 +131,13 @@ PQ3D_EXPORT int pq3d_snapshot(int nf, const double *const *fields, const int64_t
     PQ3D_CHECK(cudaGetDevice(&dev));
     PQ3D_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int64_t need = (n + SNAP_THREADS - 1) / SNAP_THREADS;
-    const int grid = (int)(need < 4 * (int64_t)sms ? need : 4 * (int64_t)sms);
-    k_snapshot<<<grid, SNAP_THREADS, 0, side>>>(F, nf, iperm, n, out_dev);
+    const int grid = (int)(need < (int64_t)sms ? need : (int64_t)sms);
+    k_snapshot<<<grid, SNAP_THREADS, 0, side>>>(F, nf, iperm, n, d_stage);
     PQ3D_CHECK(cudaGetLastError());
+    PQ3D_CHECK(cudaEventRecord((cudaEvent_t)gathered, side));
+    PQ3D_CHECK(cudaStreamWaitEvent(compute, (cudaEvent_t)gathered, 0));
+    PQ3D_CHECK(cudaMemcpyAsync(host_out, d_stage, (size_t)nf * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
+                               side));
     PQ3D_CHECK(cudaEventRecord((cudaEvent_t)done, side));
-    PQ3D_CHECK(cudaStreamWaitEvent(compute, (cudaEvent_t)done, 0));
     return PQ3D_OK;
 }

@@ -633,32 +633,37 @@ class DeviceStepper:
 
     def snapshot_async(self, names):
         """Start copying state vectors (element order) to host memory without holding
-        up the next step.  One gather kernel on a side stream writes them straight
-        into mapped host memory, after the step that produced them (the step event
-        when no launch came since) and concurrently with the pre-launched H-matvec;
-        the next step kernel waits for it.  Two buffers alternate.  Returns (event,
-        {name: float64 array}); the arrays are valid once event.synchronize() returns
-        and stay valid until the snapshot after next (the buffer is then reused)."""
+        up the next step.  On a high-priority side stream, after the step that
+        produced them (the step event when no launch came since): one gather kernel
+        into a device staging buffer, which runs between the waves of the
+        pre-launched H-matvec, then a copy-engine transfer to pinned host memory.
+        The next step kernel waits for the gather only.  Two buffers alternate.
+        Returns (event, {name: float64 array}); the arrays are valid once
+        event.synchronize() returns and stay valid until the snapshot after next
+        (the buffer is then reused)."""
         torch = self.torch
         L = self.L
         names = tuple(names)
         S = self._snap
         if S is None or S["names"] != names:
             n, nf = self.n, len(names)
-            hosts, views, devs, events = [], [], [], []
+            hosts, views, events = [], [], []
             for _ in range(2):
-                h, d, ev = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+                h, d = ctypes.c_void_p(), ctypes.c_void_p()
                 check(L.pq3d_host_map_alloc(nf * n * 8, ctypes.byref(h), ctypes.byref(d)), "pq3d_host_map_alloc")
                 hosts.append(h.value)
-                devs.append(d.value)
-                check(L.pq3d_event_create(ctypes.byref(ev)), "pq3d_event_create")
-                events.append(ev.value)
                 a = np.ctypeslib.as_array((ctypes.c_double * (nf * n)).from_address(h.value)).reshape(nf, n)
                 views.append({nm: a[j] for j, nm in enumerate(names)})
-            S = {"names": names, "k": 0, "side": torch.cuda.Stream(device=self.op.dev),
+                for _ in range(2):
+                    ev = ctypes.c_void_p()
+                    check(L.pq3d_event_create(ctypes.byref(ev)), "pq3d_event_create")
+                    events.append(ev.value)
+            S = {"names": names, "k": 0, "side": torch.cuda.Stream(device=self.op.dev, priority=-100),
                  "iperm": torch.as_tensor(np.argsort(self.perm), dtype=torch.int64, device=self.op.dev),
                  "fields": np.array([self.t[nm].data_ptr() for nm in names], dtype=np.uint64),
-                 "dev": devs, "views": views, "done": [HostEvent(L, e) for e in events]}
+                 "stage": [torch.empty(nf * n, dtype=torch.float64, device=self.op.dev) for _ in range(2)],
+                 "host": hosts, "views": views, "gathered": events[0::2],
+                 "done": [HostEvent(L, e) for e in events[1::2]]}
             if self._snap is not None:
                 self._snap["release"]()
             S["release"] = weakref.finalize(self, _release_host_io, L, hosts, events)
@@ -666,18 +671,15 @@ class DeviceStepper:
         b = S["k"]
         S["k"] ^= 1
         compute = _lib.stream_ptr()
-        ready = None
-        if self._io is not None and self._state_event:
-            ready = self._io["step_done"]
-        else:
+        io = self._io if self._io is not None else self._host_io()
+        if not self._state_event:
             # the state is whatever the compute stream has enqueued so far
-            io = self._io if self._io is not None else self._host_io()
             check(L.pq3d_event_record(io["step_done"], compute), "pq3d_event_record")
             self._state_event = True
-            ready = io["step_done"]
         done = S["done"][b]
-        check(L.pq3d_snapshot(len(names), S["fields"].ctypes.data, S["iperm"].data_ptr(), self.n, S["dev"][b],
-                              ready, done._ev, compute, S["side"].cuda_stream), "pq3d_snapshot")
+        check(L.pq3d_snapshot(len(names), S["fields"].ctypes.data, S["iperm"].data_ptr(), self.n,
+                              S["stage"][b].data_ptr(), S["host"][b], io["step_done"], S["gathered"][b], done._ev,
+                              compute, S["side"].cuda_stream), "pq3d_snapshot")
         return done, S["views"][b]
 
     def get(self, name):
