@@ -153,7 +153,10 @@ int pq3d_rk_grid(int n);
  * Control block ctrl: [0] dttry in / dtnext out, [1] accepted h, [2] time,
  * [3] rejects this step, [4] status, [5] max|V1|, [6] max|V2|, [8] steps,
  * [9] total rejects, [10] total attempts.  A positive args.h_in is the trial
- * size instead of ctrl[0] (the host's dttry without a write to device memory). */
+ * size instead of ctrl[0] (the host's dttry without a write to device memory).
+ * Scratch in args: cand 4n doubles, blk 10 * grid + 16 doubles and bar 4
+ * unsigned (blk and bar zeroed once, before the first step; every step leaves
+ * them cleared). */
 int pq3d_rk_step(const void *args, int grid, cudaStream_t stream);
 
 /* Row-partitioned step (one fault over several GPUs, each rank owning tree-order

@@ -26,12 +26,13 @@ struct RkArgs {
     const double *a, *b, *dc, *f0, *shear_loading, *normal_loading, *vplc, *cr0, *sr0;
     double *y;           // elastic load rates (n x 3): A1 x, A2 x, B x  (Pa/s)
     double *cand;        // 4n scratch
-    double *blk;         // 10 * gridDim scratch: per-CTA maxima [0,4G), [4G,6G); reduced result at 6G
+    double *blk;         // 10 * gridDim + 16 scratch: per-CTA slip-rate maxima at [4G, 6G), the
+                         // grid maxima's three result slots (12 x u64) at 10G
     void *x;             // next deficit, interleaved (2n + padding), FP32 or FP64
     double *ctrl;        // control block (see pq3d.h)
     double *hist;        // per-step history, 6 doubles per step (may be null)
     const double *hforce; // dt replay: if non-null, step s uses h = hforce[s] and is accepted
-    unsigned *bar;       // bar[0] arrivals, bar[1] generation, bar[2] end-of-step count (zeroed once)
+    unsigned *bar;       // bar[0] arrivals, bar[2] end-of-step count (zeroed once; cleared by each step)
     const void *slots;   // when fuse_rowsum: per-row partial sums of the H-matvec
     const int32_t *leaf_of_row, *leaf_ptr, *leaf_off;
     double *ctrl_host;   // mapped host memory (may be null): ctrl[0..11) after the step, then
@@ -41,18 +42,38 @@ struct RkArgs {
     double h_in;         // > 0: the step's trial size (instead of ctrl[0])
 };
 
-// Grid-wide NaN-propagating max of four values.  Every CTA reduces its own
-// values and posts them to blk; the CTA that arrives last at the barrier reduces
-// the posted values with all its threads, publishes the result in res and then
-// releases the others (bounded spin: on timeout ctrl[4] = PQ3D_ERR_TIMEOUT and
-// false is returned).  All CTAs return the same four values.
-// bar[0]: arrival count, bar[1]: generation, bar[2]: end-of-step count.
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned atom_add_acq_rel_u32(unsigned *p, unsigned x)
+{
+    unsigned old;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(x) : "memory");
+    return old;
+}
+
+// Grid-wide NaN-propagating max of four values that are >= 0 or +NaN, in one
+// phase.  Every CTA folds its block maximum into a result slot with 64-bit
+// atomicMax on the bit patterns (for such values the unsigned order of the
+// bits is the order of the values, and +NaN lies above +inf, so the fold is
+// nanmax), then arrives on bar[0] with acquire-release semantics; a CTA goes on
+// once bar[0] reaches (attempt + 1) * gridDim.x and reads the slot.  Attempts
+// rotate over three slots of four: the CTA that arrives last at attempt a
+// clears slot (a + 2) % 3, which every CTA finished reading before it arrived
+// at a and which no CTA touches before the next barrier.  The last CTA to
+// finish the step clears bar[0] and the slots.  All CTAs return the same four
+// values.  Bounded spin: on timeout ctrl[4] = PQ3D_ERR_TIMEOUT and false is
+// returned.
 template <int NT>
-__device__ bool grid_max4(double *v, double *blk, double *res, unsigned *bar, double *ctrl)
+__device__ bool grid_max4(double *v, unsigned long long *slots3, unsigned *bar, int attempt, double *ctrl)
 {
     __shared__ double wred[NT / 32][4];
-    __shared__ int s_last;
-    __shared__ unsigned s_gen;
+    __shared__ double s_res[4];
+    __shared__ int s_ok;
 #pragma unroll
     for (int q = 0; q < 4; ++q)
 #pragma unroll
@@ -62,58 +83,34 @@ __device__ bool grid_max4(double *v, double *blk, double *res, unsigned *bar, do
         for (int q = 0; q < 4; ++q) wred[threadIdx.x >> 5][q] = v[q];
     __syncthreads();
     if (threadIdx.x == 0) {
+        unsigned long long *r = slots3 + 4 * (attempt % 3);
         double w[4] = {wred[0][0], wred[0][1], wred[0][2], wred[0][3]};
         for (int k = 1; k < NT / 32; ++k)
             for (int q = 0; q < 4; ++q) w[q] = nanmax(w[q], wred[k][q]);
-        for (int q = 0; q < 4; ++q) blk[(int64_t)q * gridDim.x + blockIdx.x] = w[q];
-        s_gen = *(volatile unsigned *)(bar + 1);
-        __threadfence();
-        s_last = atomicAdd(bar, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    bool ok = true;
-    if (s_last) {
-        __threadfence();
-        double m[4] = {0, 0, 0, 0};
-        for (unsigned k = threadIdx.x; k < gridDim.x; k += NT)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) m[q] = nanmax(m[q], __ldcg(blk + (int64_t)q * gridDim.x + k));
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) m[q] = nanmax(m[q], __shfl_down_sync(0xffffffffu, m[q], o));
-        __syncthreads();
-        if ((threadIdx.x & 31) == 0)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) wred[threadIdx.x >> 5][q] = m[q];
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int q = 0; q < 4; ++q) {
-                double w = wred[0][q];
-                for (int k = 1; k < NT / 32; ++k) w = nanmax(w, wred[k][q]);
-                __stcg(res + q, w);
+        for (int q = 0; q < 4; ++q) atomicMax(r + q, (unsigned long long)__double_as_longlong(w[q]));
+        const unsigned target = (unsigned)(attempt + 1) * gridDim.x;
+        int ok = 1;
+        if (atom_add_acq_rel_u32(bar, 1u) + 1u == target) {
+            unsigned long long *z = slots3 + 4 * ((attempt + 2) % 3);
+            for (int q = 0; q < 4; ++q) __stcg(z + q, 0ull);
+        } else {
+            long long it = 0;
+            while (ld_acquire_u32(bar) < target) {
+                if (++it > (1LL << 24)) {
+                    ctrl[4] = (double)PQ3D_ERR_TIMEOUT;
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
             }
-            __threadfence();
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
         }
-    } else if (threadIdx.x == 0) {
-        long long it = 0;
-        while (*(volatile unsigned *)(bar + 1) == s_gen) {
-            if (++it > (1LL << 24)) {
-                ctrl[4] = (double)PQ3D_ERR_TIMEOUT;
-                ok = false;
-                break;
-            }
-            __nanosleep(64);
-        }
-        __threadfence();
+        for (int q = 0; q < 4; ++q) s_res[q] = __longlong_as_double((long long)__ldcg(r + q));
+        s_ok = ok;
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < 4; ++q) v[q] = __ldcg(res + q);
-    return __syncthreads_and(ok);
+    for (int q = 0; q < 4; ++q) v[q] = s_res[q];
+    return s_ok != 0;
 }
 
 #ifndef PQ3D_RK_THREADS
@@ -135,8 +132,9 @@ __global__ void __launch_bounds__(RK_THREADS, PQ3D_RK_MINB) k_rk_step(RkArgs A)
     const int64_t tid0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (A.fuse_rowsum) {
         // the H-matvec's row reduction (k_rowsum) done here: y[i] = sum of row i's slots
-        for (int64_t i = tid0; i < n; i += stride) fused_rowsum(A, i);
+        for (int64_t base = (int64_t)blockIdx.x * RK_THREADS; base < n; base += stride) rowsum_cta<RK_THREADS>(A, base);
     }
+    unsigned long long *slots3 = (unsigned long long *)(A.blk + 10 * (int64_t)gridDim.x);
     const bool forced = A.hforce != nullptr;
     StepCtl c{forced ? A.hforce[A.step_index] : (A.h_in > 0.0 ? A.h_in : A.ctrl[0]), 0.0, 0, 0, false};
     c.dtnext = c.h;
@@ -153,7 +151,7 @@ __global__ void __launch_bounds__(RK_THREADS, PQ3D_RK_MINB) k_rk_step(RkArgs A)
         }
         // grid-wide maxima of (m1, g1, g2, g3); identical in every CTA
         double E[4] = {m1, g1, g2, g3};
-        if (!grid_max4<RK_THREADS>(E, A.blk, A.blk + 6 * (int64_t)gridDim.x, A.bar, A.ctrl)) return;
+        if (!grid_max4<RK_THREADS>(E, slots3, A.bar, c.attempt, A.ctrl)) return;
         if (controller(c, E, A.reltol, forced)) break;
     }
     const double h = c.h, dtnext = c.dtnext;
@@ -209,6 +207,8 @@ __global__ void __launch_bounds__(RK_THREADS, PQ3D_RK_MINB) k_rk_step(RkArgs A)
         w2 = vred[0][1];
         for (int k = 1; k < RK_THREADS / 32; ++k) { w1 = fmax(w1, vred[k][0]); w2 = fmax(w2, vred[k][1]); }
         A.bar[2] = 0u;
+        A.bar[0] = 0u;
+        for (int q = 0; q < 12; ++q) slots3[q] = 0ull;
         if (accepted) {
             const double t = A.ctrl[2] + h;
             A.ctrl[2] = t;
@@ -394,7 +394,7 @@ PQ3D_EXPORT int pq3d_rk_step(const void *args, int grid, cudaStream_t stream)
 #define PQ3D_NOALLOC_MAX_N 131072
 #define PQ3D_NOALLOC_MAX_GRID 4096   // CTAs of RK_THREADS threads
 
-static __device__ __align__(256) double g_rk_scratch[4 * PQ3D_NOALLOC_MAX_N + 10 * PQ3D_NOALLOC_MAX_GRID + 2];
+static __device__ __align__(256) double g_rk_scratch[4 * PQ3D_NOALLOC_MAX_N + 10 * PQ3D_NOALLOC_MAX_GRID + 16 + 2];
 
 #include <mutex>
 #include <stdio.h>
@@ -440,9 +440,11 @@ PQ3D_EXPORT int pq3d_rk_step_noalloc(const void *args, int grid, cudaStream_t st
     if (rc != PQ3D_OK) return rc;
     A.cand = s;
     A.blk = s + 4 * (size_t)PQ3D_NOALLOC_MAX_N;
-    A.bar = (unsigned *)(s + 4 * (size_t)PQ3D_NOALLOC_MAX_N + 10 * (size_t)PQ3D_NOALLOC_MAX_GRID);
-    // the barrier counters must start at zero; the rest is written before it is read
+    A.bar = (unsigned *)(s + 4 * (size_t)PQ3D_NOALLOC_MAX_N + 10 * (size_t)PQ3D_NOALLOC_MAX_GRID + 16);
+    // the barrier counters and the grid maxima's result slots (at blk + 10 * grid)
+    // must start at zero; the rest is written before it is read
     PQ3D_CHECK(cudaMemsetAsync(A.bar, 0, 4 * sizeof(unsigned), stream));
+    PQ3D_CHECK(cudaMemsetAsync(A.blk + 10 * (size_t)grid, 0, 12 * sizeof(unsigned long long), stream));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid);
     cfg.blockDim = dim3(RK_THREADS);

@@ -107,6 +107,82 @@ __device__ __forceinline__ void fused_rowsum(const A &S, int64_t i)
     S.y[3 * i + 2] = a2;
 }
 
+// fused_rowsum for the CTA's rows [base, base + NT), with all NT threads of the
+// CTA taking part (call from every thread).  The leaf_off range of the CTA's
+// leaves is contiguous (leaves are numbered in row order), so it is staged in
+// shared memory once; then every thread sums its row's slots in list order (the
+// same sums as fused_rowsum) with eight list entries of loads in flight.
+constexpr int RS_STAGE = 2048;   // staged leaf_off entries per CTA (larger ranges read them from global)
+
+template <int NT, class A>
+__device__ __forceinline__ void rowsum_cta(const A &S, int64_t base)
+{
+    __shared__ int s_off[RS_STAGE];
+    __shared__ int s_kb, s_ke;
+    const int64_t n = S.n;
+    const int64_t i = base + threadIdx.x;
+    const int64_t last = (base + NT < n ? base + NT : n) - 1;
+    int k0 = 0, k1 = 0;
+    if (i < n) {
+        const int l = S.leaf_of_row[i];
+        k0 = S.leaf_ptr[l];
+        k1 = S.leaf_ptr[l + 1];
+    }
+    if (threadIdx.x == 0) s_kb = k0;
+    if (i == last) s_ke = k1;
+    __syncthreads();
+    const int kb = s_kb, ke = s_ke;
+    const bool staged = ke - kb <= RS_STAGE;
+    if (staged)
+        for (int k = kb + (int)threadIdx.x; k < ke; k += NT) s_off[k - kb] = __ldg(S.leaf_off + k);
+    __syncthreads();
+    if (i < n) {
+        double a0 = 0, a1 = 0, a2 = 0;
+        int k = k0;
+        if (S.slots_fp32) {
+            const float *sl = (const float *)S.slots;
+            for (; k + 8 <= k1; k += 8) {
+                float v[24];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int off = staged ? s_off[k + u - kb] : __ldg(S.leaf_off + k + u);
+                    const int64_t s = 3 * ((int64_t)off + i);
+                    v[3 * u] = __ldcg(sl + s); v[3 * u + 1] = __ldcg(sl + s + 1); v[3 * u + 2] = __ldcg(sl + s + 2);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) { a0 += (double)v[3 * u]; a1 += (double)v[3 * u + 1]; a2 += (double)v[3 * u + 2]; }
+            }
+            for (; k < k1; ++k) {
+                const int off = staged ? s_off[k - kb] : __ldg(S.leaf_off + k);
+                const int64_t s = 3 * ((int64_t)off + i);
+                a0 += (double)__ldcg(sl + s); a1 += (double)__ldcg(sl + s + 1); a2 += (double)__ldcg(sl + s + 2);
+            }
+        } else {
+            const double *sl = (const double *)S.slots;
+            for (; k + 8 <= k1; k += 8) {
+                double v[24];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int off = staged ? s_off[k + u - kb] : __ldg(S.leaf_off + k + u);
+                    const int64_t s = 3 * ((int64_t)off + i);
+                    v[3 * u] = __ldcg(sl + s); v[3 * u + 1] = __ldcg(sl + s + 1); v[3 * u + 2] = __ldcg(sl + s + 2);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) { a0 += v[3 * u]; a1 += v[3 * u + 1]; a2 += v[3 * u + 2]; }
+            }
+            for (; k < k1; ++k) {
+                const int off = staged ? s_off[k - kb] : __ldg(S.leaf_off + k);
+                const int64_t s = 3 * ((int64_t)off + i);
+                a0 += __ldcg(sl + s); a1 += __ldcg(sl + s + 1); a2 += __ldcg(sl + s + 2);
+            }
+        }
+        S.y[3 * i] = a0;
+        S.y[3 * i + 1] = a1;
+        S.y[3 * i + 2] = a2;
+    }
+    __syncthreads();   // s_off is reused for the CTA's next rows
+}
+
 // One DP5(4) attempt of size h for element i (RungeKutte_solve_Dormand_Prince,
 // src/QDsim.py:1001-1134) with the frozen load y[i] and start-of-step slip rate:
 // the 5th-order candidate goes to cand (Tno, Tt1o, Tt2o, psi planes of n), the

@@ -471,7 +471,7 @@ class DeviceStepper:
         self.grid = self.L.pq3d_rk_grid(n)
         if self.grid <= 0:
             raise _lib.Pq3dError("pq3d_rk_grid failed")
-        self.blk = torch.zeros(10 * self.grid, **f64)
+        self.blk = torch.zeros(10 * self.grid + 16, **f64)     # per-CTA maxima + grid-max result slots
         self.ctrl = torch.zeros(16, **f64)
         self.bar = torch.zeros(4, dtype=torch.int32, device=dev)
         self.hist = None
