@@ -581,8 +581,8 @@ def main():
     e2e = {"value": ne * world / t_e2e, "unit": "steps/s", "h2d_bytes_per_step": 8,
            "d2h_bytes_per_step": int(12 * 8 + 2 * 8 * sim.xg.shape[0]), "steps": ne,
            "path": "QDsim.simu_forward per step (control block to mapped host memory; the next step's "
-                   "H-matvec enqueued before the host waits) + slip-rate and traction vectors to mapped "
-                   "host memory (QDsim.snapshot_async: gather kernel on a side stream)"}
+                   "H-matvec enqueued before the host waits) + slip-rate and traction vectors to pinned "
+                   "host memory (QDsim.snapshot_async: gather on a side stream, copy-engine transfer)"}
 
     # CPU baseline: the reference's step on the same operator (rank 0, N=1)
     cpu = None
