@@ -239,14 +239,16 @@ int pq3d_event_query(void *ev);
  * pointers, n doubles each) into host memory host_out (nf x n, element order:
  * host_out[j][e] = fields[j][iperm[e]]) through the device staging buffer
  * d_stage (nf x n).  On `side`, after `ready` (may be NULL): gather, record
- * `gathered` (and make `compute` wait for it, so a step enqueued later on
- * `compute` cannot overwrite the vectors before they are read), copy to
+ * `gathered` (and, when compute_waits, make `compute` wait for it, so a step
+ * enqueued later on `compute` cannot overwrite the vectors before they are
+ * read; otherwise the caller does so with pq3d_stream_wait_event), copy to
  * host_out, record `done`.  With RkArgs.ctrl_host set (mapped memory, 16
  * doubles), pq3d_rk_step also stores ctrl[0..11) there and then
  * ctrl_host[15] = step_index + 1. */
 int pq3d_snapshot(int nf, const double *const *fields, const int64_t *iperm, int64_t n, double *d_stage,
                   double *host_out, void *ready, void *gathered, void *done, cudaStream_t compute,
-                  cudaStream_t side);
+                  cudaStream_t side, int compute_waits);
+int pq3d_stream_wait_event(cudaStream_t stream, void *ev);
 
 #ifdef __cplusplus
 }

@@ -108,7 +108,8 @@ def load():
     for f in ("pq3d_event_destroy", "pq3d_event_sync", "pq3d_event_query"):
         getattr(L, f).argtypes = [vp]
     L.pq3d_event_record.argtypes = [vp, vp]
-    L.pq3d_snapshot.argtypes = [i32, vp, vp, i64, vp, vp, vp, vp, vp, vp, vp]
+    L.pq3d_snapshot.argtypes = [i32, vp, vp, i64, vp, vp, vp, vp, vp, vp, vp, i32]
+    L.pq3d_stream_wait_event.argtypes = [vp, vp]
     L.pq3d_ens_args_bytes.restype = ctypes.c_size_t
     L.pq3d_ens_grid.argtypes = [i32]
     L.pq3d_ens_step.argtypes = [vp, i32, vp]
@@ -116,7 +117,7 @@ def load():
               "pq3d_aca_batched", "pq3d_aca_pack", "pq3d_hmatvec", "pq3d_rk_grid", "pq3d_rk_step", "pq3d_ens_grid",
               "pq3d_ens_step", "pq3d_ens_task_rows", "pq3d_rk_rows_attempt", "pq3d_rk_rows_accept",
               "pq3d_host_map_alloc", "pq3d_host_map_free", "pq3d_event_create", "pq3d_event_destroy",
-              "pq3d_event_record", "pq3d_event_sync", "pq3d_event_query", "pq3d_snapshot"):
+              "pq3d_event_record", "pq3d_event_sync", "pq3d_event_query", "pq3d_snapshot", "pq3d_stream_wait_event"):
         getattr(L, f).restype = ctypes.c_int
     sizes = {"DenseItem": (L.pq3d_item_bytes(0), DENSE_ITEM.itemsize), "VItem": (L.pq3d_item_bytes(1), V_ITEM.itemsize),
              "UTask": (L.pq3d_item_bytes(2), U_TASK.itemsize),

@@ -114,10 +114,12 @@ PQ3D_EXPORT int pq3d_event_query(void *ev)
 // cannot overwrite the state before it is read, but does not wait for the
 // transfer; the copy engine then moves d_stage to host_out and `done` is
 // recorded.  host_out is complete once `done` has completed.  d_stage and
-// host_out must not be reused before `done`.
+// host_out must not be reused before `done`.  With compute_waits = 0 the caller
+// makes `compute` wait for `gathered` itself (pq3d_stream_wait_event), e.g. after
+// enqueueing work that does not write the gathered vectors.
 PQ3D_EXPORT int pq3d_snapshot(int nf, const double *const *fields, const int64_t *iperm, int64_t n, double *d_stage,
                               double *host_out, void *ready, void *gathered, void *done, cudaStream_t compute,
-                              cudaStream_t side)
+                              cudaStream_t side, int compute_waits)
 {
     if (nf <= 0 || nf > SNAP_MAX_FIELDS || !fields || !iperm || n <= 0 || !d_stage || !host_out || !gathered || !done)
         return PQ3D_ERR_ARG;
@@ -135,9 +137,16 @@ PQ3D_EXPORT int pq3d_snapshot(int nf, const double *const *fields, const int64_t
     k_snapshot<<<grid, SNAP_THREADS, 0, side>>>(F, nf, iperm, n, d_stage);
     PQ3D_CHECK(cudaGetLastError());
     PQ3D_CHECK(cudaEventRecord((cudaEvent_t)gathered, side));
-    PQ3D_CHECK(cudaStreamWaitEvent(compute, (cudaEvent_t)gathered, 0));
+    if (compute_waits) PQ3D_CHECK(cudaStreamWaitEvent(compute, (cudaEvent_t)gathered, 0));
     PQ3D_CHECK(cudaMemcpyAsync(host_out, d_stage, (size_t)nf * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
                                side));
     PQ3D_CHECK(cudaEventRecord((cudaEvent_t)done, side));
+    return PQ3D_OK;
+}
+
+PQ3D_EXPORT int pq3d_stream_wait_event(cudaStream_t stream, void *ev)
+{
+    if (!ev) return PQ3D_ERR_ARG;
+    PQ3D_CHECK(cudaStreamWaitEvent(stream, (cudaEvent_t)ev, 0));
     return PQ3D_OK;
 }

@@ -60,7 +60,58 @@ def _flag(p, key, default=False):
     return p.get(key, "True" if default else "False") == "True"
 
 
+# QDsim state vectors (reference attribute name -> device field name)
+_STATE = {"Tno": "Tno", "Tt1o": "Tt1o", "Tt2o": "Tt2o", "state": "psi", "slip1": "slip1", "slip2": "slip2",
+          "slipv1": "slipv1", "slipv2": "slipv2", "slipv": "slipv", "rake": "rake", "Tt": "Tt", "fric": "fric",
+          "slip": "slip"}
+
+
+class _DeviceState:
+    """A QDsim state vector under the reference's attribute name.  Until the device
+    steps it is the host array; after simu_forward the first read of the attribute
+    fetches the device's current values (element order), so the reference main
+    loop's per-step reads (np.max(np.abs(sim0.slipv1)), SLIPV.append(sim0.slipv),
+    src/main.py:168-184) see the step just taken.  Vectors read after one step are
+    gathered by the next step as soon as it ends (DeviceStepper.step prefetch),
+    so a loop that reads the same attributes every step waits only for a copy
+    already in flight."""
+
+    def __set_name__(self, owner, name):
+        self.name = name
+        self.key = "_h_" + name
+
+    def __get__(self, obj, owner=None):
+        if obj is None:
+            return self
+        stale = obj.__dict__.get("_stale")
+        if stale and self.name in stale:
+            obj.__dict__[self.key] = obj._dev.read_field(_STATE[self.name])
+            stale.discard(self.name)
+            obj._reads.add(self.name)
+        return obj.__dict__[self.key]
+
+    def __set__(self, obj, value):
+        obj.__dict__[self.key] = value
+        stale = obj.__dict__.get("_stale")
+        if stale:
+            stale.discard(self.name)
+
+
 class QDsim:
+    Tno = _DeviceState()
+    Tt1o = _DeviceState()
+    Tt2o = _DeviceState()
+    state = _DeviceState()
+    slip1 = _DeviceState()
+    slip2 = _DeviceState()
+    slipv1 = _DeviceState()
+    slipv2 = _DeviceState()
+    slipv = _DeviceState()
+    rake = _DeviceState()
+    Tt = _DeviceState()
+    fric = _DeviceState()
+    slip = _DeviceState()
+
     def __init__(self, elelst, nodelst, fnamePara, device="cuda", precision=None):
         i = fnamePara.rfind("/")
         self.dirname = fnamePara[:i] if i != -1 else fnamePara
@@ -304,10 +355,14 @@ class QDsim:
         return self._dev
 
     def simu_forward(self, dttry):
-        """One time step (one operator application, adaptive DP5(4)); returns (h, dtnext)."""
+        """One time step (one operator application, adaptive DP5(4)); returns (h, dtnext).
+        The state attributes (slipv, Tt, ...) read after it hold the new step's values."""
         st = self._ensure_device()
-        h, dtnext = st.step(dttry)
+        reads = self.__dict__.get("_reads") or set()
+        self._reads = set()
+        h, dtnext = st.step(dttry, prefetch=tuple(sorted(_STATE[k] for k in reads)))
         self.time = st.time
+        self._stale = set(_STATE)
         return h, dtnext
 
     def snapshot_async(self, names=("slipv", "Tt")):
@@ -439,6 +494,7 @@ class _StepGraph:
     def replay(self):
         self.plan["slots_owner"] = None
         self.stepper._state_event = False
+        self.stepper._prefetched = None
         self.graph.replay()
 
 
@@ -481,7 +537,8 @@ class DeviceStepper:
         self._token = object()          # plan["slots_owner"]: whose products the slots hold
         self._io = None                 # mapped control block and step event (step())
         self._state_event = False       # step_done marks the current state (no launch since)
-        self._snap = None
+        self._snaps = {}                # snapshot buffers per tuple of names
+        self._prefetched = None         # (done event, views) of the last step's prefetch
         self.x = op.new_x(precision)
         from .hmatrix import pack_x
         x0 = pack_x((sim.slipv1 - sim.slipvC * np.cos(sim.rake0))[self.perm],
@@ -527,6 +584,7 @@ class DeviceStepper:
     def _rk(self, step_index, h_in, stream=None, ctrl_host=0):
         """Enqueue the step kernel alone (the slots must hold the products of x)."""
         self._state_event = False
+        self._prefetched = None
         self.args["step_index"] = step_index
         self.args["h_in"] = h_in
         self.args["ctrl_host"] = ctrl_host
@@ -546,7 +604,7 @@ class DeviceStepper:
         self.hforce = h.to(dtype=self.torch.float64).contiguous()
         self.hforce_cap = self.hforce.numel()
 
-    def step(self, dttry):
+    def step(self, dttry, prefetch=()):
         """One step from the host (QDsim.simu_forward): returns (h, dtnext).
 
         The H-matvec needs only the deficit x, not the step size, so the products of
@@ -557,7 +615,9 @@ class DeviceStepper:
         so the host waits on an event and reads it without a copy.  The operator's
         slots are shared by every stepper of this precision: any other matvec into
         them, or a graph replay, clears the plan's slots_owner, and the products are
-        then computed again here."""
+        then computed again here.  prefetch names state vectors to snapshot as soon
+        as the step ends (before the next matvec is enqueued, so the gather does not
+        queue behind it); read_field then returns them."""
         io = self._io if self._io is not None else self._host_io()
         L = self.L
         P = self.op.plan(self.precision)
@@ -567,8 +627,13 @@ class DeviceStepper:
         self._rk(self.steps, float(dttry), stream, ctrl_host=io["ctrl_dev"])
         check(L.pq3d_event_record(io["step_done"], stream), "pq3d_event_record")
         self._state_event = True                      # step_done marks the state of this step
+        pre = self._snapshot(prefetch, compute_waits=False) if prefetch else None
         self.op.matvec(self.x, self.precision, slots_only=True)   # products for the next step
         P["slots_owner"] = self._token
+        if pre is not None:
+            # only the next step kernel (which writes the state) waits for the gather
+            check(L.pq3d_stream_wait_event(stream, pre[2]), "pq3d_stream_wait_event")
+            self._prefetched = (pre[0], pre[1])
         check(L.pq3d_event_sync(io["step_done"]), "pq3d_event_sync")
         c = io["ctrl"]
         if c[15] != self.steps + 1:
@@ -641,11 +706,16 @@ class DeviceStepper:
         Returns (event, {name: float64 array}); the arrays are valid once
         event.synchronize() returns and stay valid until the snapshot after next
         (the buffer is then reused)."""
+        done, views, _ = self._snapshot(names)
+        return done, views
+
+    def _snapshot(self, names, compute_waits=True):
+        """snapshot_async; also returns the raw `gathered` event."""
         torch = self.torch
         L = self.L
         names = tuple(names)
-        S = self._snap
-        if S is None or S["names"] != names:
+        S = self._snaps.get(names)
+        if S is None:
             n, nf = self.n, len(names)
             hosts, views, events = [], [], []
             for _ in range(2):
@@ -664,10 +734,8 @@ class DeviceStepper:
                  "stage": [torch.empty(nf * n, dtype=torch.float64, device=self.op.dev) for _ in range(2)],
                  "host": hosts, "views": views, "gathered": events[0::2],
                  "done": [HostEvent(L, e) for e in events[1::2]]}
-            if self._snap is not None:
-                self._snap["release"]()
             S["release"] = weakref.finalize(self, _release_host_io, L, hosts, events)
-            self._snap = S
+            self._snaps[names] = S
         b = S["k"]
         S["k"] ^= 1
         compute = _lib.stream_ptr()
@@ -679,8 +747,25 @@ class DeviceStepper:
         done = S["done"][b]
         check(L.pq3d_snapshot(len(names), S["fields"].ctypes.data, S["iperm"].data_ptr(), self.n,
                               S["stage"][b].data_ptr(), S["host"][b], io["step_done"], S["gathered"][b], done._ev,
-                              compute, S["side"].cuda_stream), "pq3d_snapshot")
-        return done, S["views"][b]
+                              compute, S["side"].cuda_stream, 1 if compute_waits else 0), "pq3d_snapshot")
+        return done, S["views"][b], S["gathered"][b]
+
+    def fetch(self, names):
+        """Element-order copies of state vectors as the last step left them, waiting
+        for the snapshot only (not for work enqueued after the step)."""
+        done, v = self.snapshot_async(names)
+        done.synchronize()
+        return {k: np.array(v[k]) for k in names}
+
+    def read_field(self, name):
+        """One state vector (element order, a new array) as the last step left it:
+        from that step's prefetch when it holds the vector and nothing was launched
+        since, else by a snapshot of its own."""
+        pf = self._prefetched
+        if pf is not None and name in pf[1]:
+            pf[0].synchronize()
+            return np.array(pf[1][name])
+        return self.fetch((name,))[name]
 
     def get(self, name):
         v = self.t[name].cpu().numpy()

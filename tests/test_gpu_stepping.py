@@ -120,3 +120,29 @@ def test_snapshot_after_other_launches(tiny):
     for _ in range(3):
         _, d = st.step(d)
         check_snapshot()
+
+
+def test_reference_loop_reads_current_state(lib, tiny_files):
+    """The reference main loop reads sim0.slipv1, sim0.slipv2, sim0.slipv and sim0.Tt
+    after every simu_forward (src/main.py:168-184).  Those attributes hold the step
+    just taken: equal to the device state read back synchronously, distinct arrays
+    per step, and max |V1|, max |V2| equal to the step kernel's own maxima."""
+    from pyquake3d_b200 import QDsim, read_mshV2
+    nodes, tris = read_mshV2(tiny_files[0])
+    sim = QDsim(tris, nodes, tiny_files[1])
+    v0 = sim.slipv.copy()
+    dttry = sim.htry
+    slipv_hist = []
+    for i in range(6):
+        dttry, dtnext = sim.simu_forward(dttry)
+        st = sim._dev
+        m1, m2 = np.max(np.abs(sim.slipv1)), np.max(np.abs(sim.slipv2))
+        c = st.ctrl.cpu().numpy()
+        assert m1 == c[5] and m2 == c[6], i
+        for name, dev in (("slipv", "slipv"), ("Tt", "Tt"), ("state", "psi"), ("slip", "slip")):
+            assert np.array_equal(getattr(sim, name), st.get(dev)), (i, name)
+        slipv_hist.append(sim.slipv)
+        dttry = dtnext
+    assert not np.array_equal(slipv_hist[0], v0)
+    assert not np.array_equal(slipv_hist[0], slipv_hist[-1])
+    assert len({id(a) for a in slipv_hist}) == len(slipv_hist)
