@@ -13,14 +13,16 @@ rank owns a contiguous range of tree-order ROWS instead:
   * cuts balance the matvec bytes of each rank (dense entries of its rows, U
     rows and V of its low-rank blocks);
   * a rank computes y only for its rows and steps only its rows; the one data
-    exchange per step is the slip-rate deficit x (each rank contributes its
-    rows: a sum over ranks of vectors with disjoint support), and every DP5(4)
-    attempt reduces four error maxima (max over ranks, NaN flags carried
-    separately so NaN propagates as in the reference).  No reduce of y.
+    exchange per step is an all-gather of the slip-rate deficit (each rank
+    contributes its rows, 2 (r1 - r0) values in tree order, (x1, x2)
+    interleaved; ranks own consecutive row ranges, so the gathered pieces in
+    rank order are the whole deficit), and every DP5(4) attempt reduces four
+    error maxima (max over ranks, NaN flags carried separately so NaN
+    propagates as in the reference).  No reduce of y.
 
 The step orchestration (PartitionedStepper) is written against two small
 interfaces: a backend per local rank (matvec, attempt over its rows, accept)
-and a communicator (sum / max over all ranks).  DeviceRowBackend runs the
+and a communicator (gather / max over all ranks).  DeviceRowBackend runs the
 libpq3d.so row-range kernels; TorchComm reduces over torch.distributed ranks
 (and over several local backends, which is how two ranks are emulated on one
 GPU without kernels that wait on each other).
@@ -171,8 +173,8 @@ class RankStructure:
 
 
 class TorchComm:
-    """Sum / max over the local backends' tensors, then over torch.distributed
-    ranks (when a process group is given or initialized)."""
+    """Gather / sum / max over the local backends' tensors, then over
+    torch.distributed ranks (when a process group is given or initialized)."""
 
     def __init__(self, use_dist=None):
         import torch
@@ -191,6 +193,27 @@ class TorchComm:
         if self.use_dist:
             self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
         return t
+
+    def gather(self, parts):
+        """Concatenation, in rank order, of every rank's 1-D piece (the local
+        backends' pieces being consecutive ranks).  Across processes: one
+        all-gather of the pieces padded to the longest (the piece lengths are
+        exchanged once and kept, as the partition does not change)."""
+        torch = self.torch
+        t = parts[0] if len(parts) == 1 else torch.cat([p.to(parts[0].device) for p in parts])
+        if not self.use_dist:
+            return t.clone() if len(parts) == 1 else t
+        sizes = getattr(self, "_sizes", None)
+        if sizes is None or sizes[self.dist.get_rank()] != t.numel():
+            n = torch.tensor([t.numel()], dtype=torch.int64, device=t.device)
+            out = [torch.zeros_like(n) for _ in range(self.dist.get_world_size())]
+            self.dist.all_gather(out, n)
+            sizes = self._sizes = [int(v.item()) for v in out]
+        m = max(sizes)
+        pad = t if t.numel() == m else torch.cat([t, t.new_zeros(m - t.numel())])
+        out = [torch.empty_like(pad) for _ in sizes]
+        self.dist.all_gather(out, pad.contiguous())
+        return torch.cat([o[:k] for o, k in zip(out, sizes)])
 
     def max(self, parts):
         t = self._local(parts, self.torch.maximum)
@@ -225,13 +248,15 @@ class PartitionedStepper:
     """QDsim.simu_forward (src/QDsim.py:892-996) over row-partitioned ranks.
 
     backends: the ranks of this process (one per GPU in a multi-process run; two
-    or more to emulate ranks in one process).  Each backend provides
-      x_part()          its rows of the slip-rate deficit (zeros elsewhere)
-      matvec(x)         H-matvec of its blocks for the global deficit x
+    or more to emulate ranks in one process), in rank order.  Each backend provides
+      x_rows()          its rows of the slip-rate deficit: 2 (r1 - r0) values,
+                        tree order, (x1, x2) interleaved
+      matvec_gathered(xt) H-matvec of its blocks for the whole deficit xt (2n
+                        values, tree order, interleaved: all ranks' pieces)
       attempt(h, first) DP5(4) attempt of size h on its rows -> 8 values:
                         4 error maxima (psi, Tt1, Tt2, Tno) with NaN -> 0, 4 NaN flags
       accept(h)         accepted-step update of its rows -> (max|V1|, max|V2|, 0, 0 flags)
-    comm: sum / max over all ranks (TorchComm)."""
+    comm: gather / max over all ranks (TorchComm)."""
 
     def __init__(self, backends, comm, reltol):
         self.backends = list(backends)
@@ -243,9 +268,9 @@ class PartitionedStepper:
         self.vmax = (0.0, 0.0)
 
     def step(self, dttry, h_forced=None):
-        x = self.comm.sum([b.x_part() for b in self.backends])
+        xt = self.comm.gather([b.x_rows() for b in self.backends])
         for b in self.backends:
-            b.matvec(x)
+            b.matvec_gathered(xt)
         h = float(dttry)
         nrjct = 0
         first = True
@@ -338,6 +363,8 @@ class DeviceRowBackend:
         keep[2 * Ps:2 * Ps + n] = mask
         keep[3 * Ps:3 * Ps + n] = mask
         self.xl = torch.tensor(np.where(keep, xs, 0.0), dtype=acc, device=dev)
+        self.xg_buf = torch.zeros_like(self.xl)       # the whole deficit, operator layout
+        self.n, self.Ps = n, Ps
         A = np.zeros(1, dtype=_lib.RK_ARGS)
         for k in self.FIELDS + self.CONST:
             A[k] = self.t[k].data_ptr()
@@ -356,11 +383,20 @@ class DeviceRowBackend:
         A["V0"], A["eta"], A["reltol"] = sim.V0, sim.mu / (2.0 * sim.Cs), sim.RelTol
         self.args = A
 
-    def x_part(self):
-        return self.xl
+    def x_rows(self):
+        """This rank's rows of the deficit: the interleaved part of its x buffer,
+        which the accept kernel writes."""
+        return self.xl[2 * self.r0:2 * self.r1]
 
-    def matvec(self, x):
-        self.op.matvec(x, self.precision, slots_only=True)
+    def matvec_gathered(self, xt):
+        """H-matvec for the whole deficit xt (tree order, interleaved): the
+        operator's layout takes the interleaved pairs and the two planes."""
+        n, P = self.n, self.Ps
+        xg = self.xg_buf
+        xg[0:2 * n].copy_(xt)
+        xg[2 * P:2 * P + n].copy_(xt[0::2])
+        xg[3 * P:3 * P + n].copy_(xt[1::2])
+        self.op.matvec(xg, self.precision, slots_only=True)
 
     def attempt(self, h, first):
         check(self.L.pq3d_rk_rows_attempt(self.args.ctypes.data, self.grid, self.r0, self.r1, float(h),

@@ -17,22 +17,27 @@ class NumpyRowBackend:
         self.op = qd_oracle.OracleOperator(geo, [(b.row.indices, b.col.indices, b.aca) for b in rs.blocks],
                                            rs.aca_starts, eps=0.01)
         self.n = len(sim.xg)
-        self.rows = np.sort(sim.tree_block.struct.perm[rs.r0:rs.r1])
+        self.perm = sim.tree_block.struct.perm
+        self.tree_rows = self.perm[rs.r0:rs.r1]          # element ids of the rank's rows, tree order
+        self.rows = np.sort(self.tree_rows)
         self.st = qd_oracle.OracleStepper(qd_oracle.sim_state(sim), None, sim.V0, sim.mu, sim.Cs, sim.RelTol,
                                           sim.fix_Tn)
         self.y5 = None
 
-    def x_part(self):
-        st, r, n = self.st, self.rows, self.n
-        out = np.zeros(2 * n)
-        out[r] = (st.slipv1 - st.slipvC * np.cos(st.rake0))[r]
-        out[n + r] = (st.slipv2 - st.slipvC * np.sin(st.rake0))[r]
+    def x_rows(self):
+        """The rank's tree-order rows of the deficit, (x1, x2) interleaved."""
+        st, e = self.st, self.tree_rows
+        out = np.empty(2 * len(e))
+        out[0::2] = (st.slipv1 - st.slipvC * np.cos(st.rake0))[e]
+        out[1::2] = (st.slipv2 - st.slipvC * np.sin(st.rake0))[e]
         return torch.tensor(out)
 
-    def matvec(self, x):
-        x = x.numpy()
+    def matvec_gathered(self, xt):
+        xt = xt.numpy()
         n, op, st = self.n, self.op, self.st
-        x1, x2 = x[:n], x[n:]
+        x1, x2 = np.empty(n), np.empty(n)
+        x1[self.perm] = xt[0::2]
+        x2[self.perm] = xt[1::2]
         sigB = op.mvm(x1, "Bs") + op.mvm(x2, "Bd")
         st.AdotV1 = op.mvm(x1, "A1s") + op.mvm(x2, "A1d")
         st.AdotV2 = op.mvm(x1, "A2s") + op.mvm(x2, "A2d")
