@@ -10,9 +10,9 @@
 // advance in lock-step attempts: a fault whose step is accepted (or given up)
 // is skipped by the later attempts of the others.
 //
-// Work is split into CTA tasks of at most ENS_THREADS rows of one fault; a task
-// is always processed by the same thread mapping, so the fused row sum of the
-// first attempt and the later attempts of a row run in the same thread.  After
+// Work is split into CTA tasks of at most ENS_THREADS rows of one fault; the
+// fused row sums of a task's rows are done by its CTA before its first attempt
+// (staged slot lists, rowsum_cta).  After
 // each attempt the last CTA to arrive reduces the per-task maxima of every
 // running fault, applies the controller, publishes the per-fault state and
 // releases the others (bounded spins; PQ3D_ERR_TIMEOUT in every fault's status).
@@ -136,9 +136,10 @@ __global__ void __launch_bounds__(ENS_THREADS) k_rk_ensemble(EnsArgs A)
                 if (__ldcg(A.fstate + (int64_t)ENS_FSTATE * s + 4) != 0.0) continue;
                 h = __ldcg(A.fstate + (int64_t)ENS_FSTATE * s);
             }
+            // the H-matvec's row sums of the task's rows (one task is at most ENS_THREADS rows)
+            if (k == 0 && A.fuse_rowsum) rowsum_cta<ENS_THREADS>(A, A.task_row[t], A.task_row[t + 1]);
             double e4[4] = {0.0, 0.0, 0.0, 0.0};
             for (int64_t i = A.task_row[t] + threadIdx.x; i < A.task_row[t + 1]; i += ENS_THREADS) {
-                if (k == 0 && A.fuse_rowsum) fused_rowsum(A, i);
                 double e[4];
                 dp54_element(A, i, h, e);
 #pragma unroll

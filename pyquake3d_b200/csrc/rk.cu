@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(RK_THREADS, PQ3D_RK_MINB) k_rk_step(RkArgs A)
     const int64_t tid0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (A.fuse_rowsum) {
         // the H-matvec's row reduction (k_rowsum) done here: y[i] = sum of row i's slots
-        for (int64_t base = (int64_t)blockIdx.x * RK_THREADS; base < n; base += stride) rowsum_cta<RK_THREADS>(A, base);
+        for (int64_t base = (int64_t)blockIdx.x * RK_THREADS; base < n; base += stride) rowsum_cta<RK_THREADS>(A, base, n);
     }
     unsigned long long *slots3 = (unsigned long long *)(A.blk + 10 * (int64_t)gridDim.x);
     const bool forced = A.hforce != nullptr;

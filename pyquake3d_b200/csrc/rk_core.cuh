@@ -107,19 +107,19 @@ __device__ __forceinline__ void fused_rowsum(const A &S, int64_t i)
     S.y[3 * i + 2] = a2;
 }
 
-// fused_rowsum for the CTA's rows [base, base + NT), with all NT threads of the
-// CTA taking part (call from every thread).  The leaf_off range of the CTA's
+// fused_rowsum for the CTA's rows [base, min(base + NT, end)), with all NT
+// threads of the CTA taking part (call from every thread).  The leaf_off range of the CTA's
 // leaves is contiguous (leaves are numbered in row order), so it is staged in
 // shared memory once; then every thread sums its row's slots in list order (the
 // same sums as fused_rowsum) with eight list entries of loads in flight.
 constexpr int RS_STAGE = 2048;   // staged leaf_off entries per CTA (larger ranges read them from global)
 
 template <int NT, class A>
-__device__ __forceinline__ void rowsum_cta(const A &S, int64_t base)
+__device__ __forceinline__ void rowsum_cta(const A &S, int64_t base, int64_t end)
 {
     __shared__ int s_off[RS_STAGE];
     __shared__ int s_kb, s_ke;
-    const int64_t n = S.n;
+    const int64_t n = end;
     const int64_t i = base + threadIdx.x;
     const int64_t last = (base + NT < n ? base + NT : n) - 1;
     int k0 = 0, k1 = 0;
