@@ -1,0 +1,165 @@
+"""GPU: the benchmark workloads at full size, through size-independent properties.
+
+The oracle cannot assemble or step 20k-60k elements in seconds, so at these
+sizes the product is checked by properties that hold at any size:
+
+* sampled rows of the H-matvec against exact rows of the operator computed with
+  the Green's-function pairs kernel (pinned to the reference's library on the
+  golden vectors): the hierarchical approximation stays within a small multiple
+  of the ACA tolerance;
+* linearity and bitwise determinism of the matvec in every storage precision;
+* stepping: a CUDA graph of steps and the same steps launched eagerly are
+  bitwise equal, and the FP32 operator's trajectory stays within the 1e-5 slip
+  target of the FP64 one on the FP64 step sizes;
+* the row-partitioned step (two ranks emulated in one process) follows the
+  fused single-GPU step at the 20k thrust workload.
+
+Workloads: curved60k (59,696 triangles, rough strike-slip fault with a branch)
+and thrust20k (20,480 triangles, 30-degree thrust), generated by
+pyquake3d_b200.meshgen with fixed seeds."""
+import numpy as np
+import pytest
+
+from pyquake3d_b200 import _lib
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return _lib.load()
+
+
+def _case(name, tmp_path_factory, precision):
+    from pyquake3d_b200 import QDsim, meshgen, read_mshV2
+    msh, para = meshgen.make_case(name, str(tmp_path_factory.mktemp(name)))
+    nodes, tris = read_mshV2(msh)
+    return QDsim(tris, nodes, para, precision=precision)
+
+
+@pytest.fixture(scope="module")
+def c60(lib, tmp_path_factory):
+    sim = _case("curved60k", tmp_path_factory, "fp32")
+    sim.tree_block.want = ("fp64", "fp32", "bf16")
+    return sim, sim.tree_block.op()
+
+
+def _exact_rows(lib, sim, rows):
+    """The six operator planes (A1s, A2s, Bs, A1d, A2d, Bd) of receivers `rows`
+    against every source, from the Green's-function pairs kernel: 6 x m x n."""
+    n = len(sim.xg)
+    f64 = dict(dtype=torch.float64, device="cuda")
+    xg, ev = torch.tensor(sim.xg, **f64), torch.tensor(sim.eleVec, **f64)
+    nodes = torch.tensor(sim.nodelst, **f64)
+    tri = torch.tensor(sim.elelst.astype(np.int64), device="cuda")
+    rec = torch.empty(n * lib.pq3d_src_record_bytes() // 8, **f64)
+    st = _lib.stream_ptr()
+    _lib.check(lib.pq3d_src_records(nodes.data_ptr(), tri.data_ptr(), n, rec.data_ptr(), st), "records")
+    m = len(rows)
+    pr = torch.tensor(np.repeat(rows, n), device="cuda")
+    pc = torch.arange(n, device="cuda").repeat(m)
+    out = torch.empty(m * n * 6, **f64)
+    _lib.check(lib.pq3d_traction_pairs(xg.data_ptr(), ev.data_ptr(), rec.data_ptr(), pr.data_ptr(), pc.data_ptr(),
+                                       m * n, sim.mu, sim.lambda_, out.data_ptr(), None, 0, st), "pairs")
+    return out.view(m, n, 6).permute(2, 0, 1)
+
+
+def test_sampled_rows_match_exact_operator(lib, c60):
+    """ACA at relative tolerance eps per block: over 48 sampled receivers, each
+    traction-rate component of the H-matvec is within 20 eps (relative L2) of
+    the product with the exact operator rows, in FP64 and FP32 storage."""
+    sim, op = c60
+    eps = float(sim.Para0.get("ACA tolerance"))
+    assert sim.Para0.get("ACA relative tolerance") == "True" and eps <= 1e-4
+    n = op.n
+    rng = np.random.default_rng(11)
+    rows = np.sort(rng.choice(n, 48, replace=False))
+    x1, x2 = rng.standard_normal((2, n)) * 1e-9
+    G = _exact_rows(lib, sim, rows)
+    X1, X2 = torch.tensor(x1, device="cuda"), torch.tensor(x2, device="cuda")
+    exact = [(G[c] @ X1 + G[c + 3] @ X2).cpu().numpy() for c in range(3)]
+    for dtype, tol in (("fp64", 20 * eps), ("fp32", 20 * eps)):
+        y = op.apply(x1, x2, dtype)
+        for c in range(3):
+            err = np.linalg.norm(y[c][rows] - exact[c]) / np.linalg.norm(exact[c])
+            assert err <= tol, (dtype, c, err)
+
+
+def test_matvec_linearity_and_determinism(c60):
+    sim, op = c60
+    n = op.n
+    rng = np.random.default_rng(12)
+    a, b = rng.standard_normal((2, 2, n)) * 1e-9
+    for dtype, tol in (("fp64", 1e-12), ("fp32", 1e-5), ("bf16", 1e-5)):
+        ya = np.array(op.apply(a[0], a[1], dtype))
+        yb = np.array(op.apply(b[0], b[1], dtype))
+        yab = np.array(op.apply(a[0] + 2 * b[0], a[1] + 2 * b[1], dtype))
+        assert np.abs(yab - (ya + 2 * yb)).max() <= tol * np.abs(yab).max(), dtype
+        assert np.array_equal(ya, np.array(op.apply(a[0], a[1], dtype))), dtype   # bitwise reproducible
+
+
+def _state(st):
+    return {k: st.t[k].cpu().numpy().copy() for k in ("slip", "slipv", "psi", "Tno", "Tt")}
+
+
+def test_graph_equals_eager_steps(c60):
+    from pyquake3d_b200.qdsim import DeviceStepper
+    sim, op = c60
+    a, b = DeviceStepper(sim, op, "fp32"), DeviceStepper(sim, op, "fp32")
+    ha = a.run(100, sim.htry)
+    g = b.capture(100)
+    assert g is not None
+    b.ctrl[0] = sim.htry
+    g.replay()
+    torch.cuda.synchronize()
+    hb = b.hist.view(-1, 6).cpu().numpy()[:100]
+    assert np.array_equal(ha, hb)
+    sa, sb = _state(a), _state(b)
+    for k in sa:
+        assert np.array_equal(sa[k], sb[k]), k
+
+
+def test_fp32_operator_within_slip_target_of_fp64(c60):
+    """On the FP64 run's step sizes (dt replay), 100 steps: slip relative L2
+    error of the FP32-operator run below the 1e-5 target."""
+    from pyquake3d_b200.qdsim import DeviceStepper
+    sim, op = c60
+    ref = DeviceStepper(sim, op, "fp64")
+    h = ref.run(100, sim.htry)[:, 0]
+    mix = DeviceStepper(sim, op, "fp32")
+    mix.set_replay(torch.tensor(h, device="cuda"))
+    mix.run(100, sim.htry)
+    s64, s32 = ref.t["slip"].cpu().numpy(), mix.t["slip"].cpu().numpy()
+    err = np.linalg.norm(s32 - s64) / np.linalg.norm(s64)
+    assert err < 1e-5, err
+    assert abs(mix.time - ref.time) <= 1e-12 * ref.time
+
+
+def test_two_ranks_follow_fused_step_thrust20k(lib, tmp_path_factory):
+    """Row partition over two ranks (emulated in one process) against the fused
+    single-GPU step on the 20k thrust fault, FP64 operator, 20 steps: the same
+    step sizes and states to 1e-9 (the ranks' row sums add the same products in
+    another order)."""
+    from pyquake3d_b200.partition import DeviceRowBackend, PartitionedStepper, TorchComm, row_partition
+    from pyquake3d_b200.qdsim import DeviceStepper
+    sim = _case("thrust20k", tmp_path_factory, "fp64")
+    op = sim.tree_block.op()
+    st = sim.tree_block.struct
+    ref = DeviceStepper(sim, op, "fp64")
+    h_ref = ref.run(20, sim.htry)[:, 0]
+    b = row_partition(st, 2)
+    backends = [DeviceRowBackend(sim, st, b[r], b[r + 1], precision="fp64") for r in range(2)]
+    ps = PartitionedStepper(backends, TorchComm(use_dist=False), sim.RelTol)
+    dt = sim.htry
+    hs = []
+    for _ in range(20):
+        h, dt = ps.step(dt)
+        hs.append(h)
+    np.testing.assert_allclose(hs, h_ref, rtol=1e-9)
+    for k in ("slip", "psi", "Tt"):
+        got = np.concatenate([be.get(k) for be in backends])
+        want = ref.t[k].cpu().numpy()
+        assert np.abs(got - want).max() <= 1e-9 * np.abs(want).max(), k
