@@ -12,11 +12,15 @@ sizes the product is checked by properties that hold at any size:
   bitwise equal, and the FP32 operator's trajectory stays within the 1e-5 slip
   target of the FP64 one on the FP64 step sizes;
 * the row-partitioned step (two ranks emulated in one process) follows the
-  fused single-GPU step at the 20k thrust workload.
+  fused single-GPU step at the 20k thrust workload;
+* plain2k (one dense FP64 block) is small enough for the oracle itself: its
+  operator rows and 50 adaptive steps against the oracle on the same operator;
+* curved120k in V-mode: the MLP-seeded and the undamped-start runs agree.
 
-Workloads: curved60k (59,696 triangles, rough strike-slip fault with a branch)
-and thrust20k (20,480 triangles, 30-degree thrust), generated by
-pyquake3d_b200.meshgen with fixed seeds."""
+Workloads: plain2k (1,936 triangles, vertical strike-slip), thrust20k (20,480
+triangles, 30-degree thrust), curved60k (59,696 triangles, rough strike-slip
+fault with a branch) and curved120k (the same geometry refined, heterogeneous
+a-b and normal stress), generated by pyquake3d_b200.meshgen with fixed seeds."""
 import numpy as np
 import pytest
 
@@ -163,3 +167,65 @@ def test_two_ranks_follow_fused_step_thrust20k(lib, tmp_path_factory):
         got = np.concatenate([be.get(k) for be in backends])
         want = ref.t[k].cpu().numpy()
         assert np.abs(got - want).max() <= 1e-9 * np.abs(want).max(), k
+
+
+def test_plain2k_device_follows_oracle_on_same_operator(lib, tmp_path_factory):
+    """plain2k at full size (1,936 triangles, one dense FP64 block): sampled rows
+    of the device-assembled operator equal the C oracle's Green's function to
+    1e-10 of each plane's scale, and 50 adaptive device steps follow the
+    oracle's simu_forward on the same operator (copied to the host): h to 1e-9,
+    state to 1e-8."""
+    import qd_oracle
+    from pyquake3d_b200.hmatrix import export_blocks
+    from pyquake3d_b200.qdsim import DeviceStepper
+    sim = _case("plain2k", tmp_path_factory, "fp64")
+    op = sim.tree_block.op()
+    blocks = export_blocks(op)
+    assert len(blocks) == 1 and blocks[0][0] == "dense"
+    _, rows, cols, M = blocks[0]
+    geo = qd_oracle.Geometry(sim.xg, sim.eleVec, sim.nodelst, sim.elelst, sim.mu, sim.lambda_)
+    pick = np.random.default_rng(13).choice(len(rows), 16, replace=False)
+    ref = geo.gf_block(rows[pick], cols, 3)
+    # planar vertical fault: the normal-stress planes B are rounding noise, so the
+    # scale of every plane is the operator's maximum
+    assert np.abs(M[:, pick, :] - ref).max() <= 1e-10 * np.abs(ref).max()
+    ho = object.__new__(qd_oracle.OracleOperator)
+    ho.blocks = blocks
+    ost = qd_oracle.OracleStepper(qd_oracle.sim_state(sim), qd_oracle.operator_mvm(ho), sim.V0, sim.mu, sim.Cs,
+                                  sim.RelTol, sim.fix_Tn)
+    dst = DeviceStepper(sim, op, "fp64")
+    dt_o = dt_d = sim.htry
+    for i in range(50):
+        h_o, dt_o = ost.simu_forward(dt_o)
+        h_d, dt_d = dst.step(dt_d)
+        assert abs(h_d - h_o) <= 1e-9 * abs(h_o), i
+    for name, dev in (("slip1", "slip1"), ("state", "psi"), ("Tno", "Tno"), ("Tt1o", "Tt1o")):
+        r = getattr(ost, name)
+        assert np.abs(dst.get(dev) - r).max() <= 1e-8 * np.abs(r).max(), name
+
+
+def test_vmode_curved120k_mlp_seed_matches_newton(lib, tmp_path_factory):
+    """curved120k at full size (V-mode with the Newton-seeding MLP): the MLP is
+    trained on the run's own logged solves; Newton judges every start, so the
+    MLP-seeded run and the undamped-start run take the same steps (time to 1e-9)
+    and reach the same slip (1e-9), with at most 1% of solves falling back."""
+    from pyquake3d_b200.vmode import MLPTrainer, VStepper
+    sim = _case("curved120k", tmp_path_factory, "fp32")
+    op = sim.tree_block.op()
+    logger = VStepper(sim, op, "fp32", seed_mode=1, log_cap=1 << 20)
+    logger.run(10, chunk=2)
+    tr = MLPTrainer(seed=0)
+    hist = tr.fit(logger.samples(), epochs=10, batch=8192, lr=3e-3)
+    assert hist[-1] < 0.2 * hist[0]
+    del logger
+    runs = {}
+    for mode in (1, 2):
+        st = VStepper(sim, op, "fp32", seed_mode=mode, mlp_params=tr.P if mode == 2 else None)
+        c = st.run(10, chunk=2)
+        runs[mode] = (c.copy(), st.get("slip1"), st.newton_stats())
+        del st
+    assert int(runs[1][0][8]) == int(runs[2][0][8]) == 10
+    np.testing.assert_allclose(runs[2][0][2], runs[1][0][2], rtol=1e-9)
+    assert np.linalg.norm(runs[2][1] - runs[1][1]) <= 1e-9 * np.linalg.norm(runs[1][1])
+    s = runs[2][2]
+    assert s["fallbacks"] <= 0.01 * s["solves"], s
