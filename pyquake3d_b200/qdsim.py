@@ -68,13 +68,15 @@ _STATE = {"Tno": "Tno", "Tt1o": "Tt1o", "Tt2o": "Tt2o", "state": "psi", "slip1":
 
 class _DeviceState:
     """A QDsim state vector under the reference's attribute name.  Until the device
-    steps it is the host array; after simu_forward the first read of the attribute
-    fetches the device's current values (element order), so the reference main
-    loop's per-step reads (np.max(np.abs(sim0.slipv1)), SLIPV.append(sim0.slipv),
-    src/main.py:168-184) see the step just taken.  Vectors read after one step are
-    gathered by the next step as soon as it ends (DeviceStepper.step prefetch),
-    so a loop that reads the same attributes every step waits only for a copy
-    already in flight."""
+    steps it is the host array; once any step kernel has run since the host copy
+    was taken (simu_forward, or bulk stepping through the DeviceStepper: run,
+    launch, graph replays), the first read of the attribute fetches the device's
+    current values (element order).  So the reference main loop's per-step reads
+    (np.max(np.abs(sim0.slipv1)), SLIPV.append(sim0.slipv), src/main.py:168-184)
+    see the step just taken.  Vectors read after one simu_forward are gathered by
+    the next one as soon as its step ends (DeviceStepper.step prefetch), so a
+    loop that reads the same attributes every step waits only for a copy already
+    in flight."""
 
     def __set_name__(self, owner, name):
         self.name = name
@@ -83,12 +85,19 @@ class _DeviceState:
     def __get__(self, obj, owner=None):
         if obj is None:
             return self
-        stale = obj.__dict__.get("_stale")
-        if stale and self.name in stale:
-            obj.__dict__[self.key] = obj._dev.read_field(_STATE[self.name])
-            stale.discard(self.name)
-            obj._reads.add(self.name)
-        return obj.__dict__[self.key]
+        d = obj.__dict__
+        dev = d.get("_dev")
+        if dev is not None:
+            key = (dev._token, dev.version)
+            if d.get("_host_key") != key:          # the device stepped since the host copies
+                d["_host_key"] = key
+                d["_stale"] = set(_STATE)
+            stale = d["_stale"]
+            if self.name in stale:
+                d[self.key] = dev.read_field(_STATE[self.name])
+                stale.discard(self.name)
+                d.setdefault("_reads", set()).add(self.name)
+        return d[self.key]
 
     def __set__(self, obj, value):
         obj.__dict__[self.key] = value
@@ -352,6 +361,8 @@ class QDsim:
     def _ensure_device(self):
         if self._dev is None:
             self._dev = DeviceStepper(self, self.tree_block.op(), self.precision)
+            self._host_key = (self._dev._token, self._dev.version)    # built from the host arrays
+            self._stale = set()
         return self._dev
 
     def simu_forward(self, dttry):
@@ -362,7 +373,6 @@ class QDsim:
         self._reads = set()
         h, dtnext = st.step(dttry, prefetch=tuple(sorted(_STATE[k] for k in reads)))
         self.time = st.time
-        self._stale = set(_STATE)
         return h, dtnext
 
     def snapshot_async(self, names=("slipv", "Tt")):
@@ -495,6 +505,7 @@ class _StepGraph:
         self.plan["slots_owner"] = None
         self.stepper._state_event = False
         self.stepper._prefetched = None
+        self.stepper.version += 1
         self.graph.replay()
 
 
@@ -535,6 +546,7 @@ class DeviceStepper:
         self.hforce = None
         self.hforce_cap = 0
         self._token = object()          # plan["slots_owner"]: whose products the slots hold
+        self.version = 0                # step kernels launched (QDsim attributes compare it)
         self._io = None                 # mapped control block and step event (step())
         self._state_event = False       # step_done marks the current state (no launch since)
         self._snaps = {}                # snapshot buffers per tuple of names
@@ -585,6 +597,7 @@ class DeviceStepper:
         """Enqueue the step kernel alone (the slots must hold the products of x)."""
         self._state_event = False
         self._prefetched = None
+        self.version += 1
         self.args["step_index"] = step_index
         self.args["h_in"] = h_in
         self.args["ctrl_host"] = ctrl_host
@@ -774,6 +787,8 @@ class DeviceStepper:
         return out
 
     def to_host(self, sim):
+        sim._host_key = (self._token, self.version)       # the host copies below are current
+        sim._stale = set()
         sim.Tno, sim.Tt1o, sim.Tt2o, sim.state = self.get("Tno"), self.get("Tt1o"), self.get("Tt2o"), self.get("psi")
         sim.slip1, sim.slip2, sim.slip = self.get("slip1"), self.get("slip2"), self.get("slip")
         sim.slipv1, sim.slipv2, sim.slipv = self.get("slipv1"), self.get("slipv2"), self.get("slipv")

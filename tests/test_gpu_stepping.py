@@ -146,3 +146,25 @@ def test_reference_loop_reads_current_state(lib, tiny_files):
     assert not np.array_equal(slipv_hist[0], v0)
     assert not np.array_equal(slipv_hist[0], slipv_hist[-1])
     assert len({id(a) for a in slipv_hist}) == len(slipv_hist)
+
+
+def test_attributes_follow_bulk_device_steps(lib, tiny_files):
+    """After bulk stepping through the DeviceStepper (run, a captured graph), the
+    QDsim attributes read the device state, without an explicit sync_to_host;
+    after sync_to_host they are the synced arrays themselves."""
+    from pyquake3d_b200 import QDsim, read_mshV2
+    nodes, tris = read_mshV2(tiny_files[0])
+    sim = QDsim(tris, nodes, tiny_files[1])
+    st = sim._ensure_device()
+    v0 = sim.slipv.copy()
+    assert np.array_equal(sim.slipv, v0)              # no step yet: the host arrays
+    st.run(5, sim.htry)
+    assert np.array_equal(sim.slipv, st.get("slipv"))
+    assert not np.array_equal(sim.slipv, v0)
+    g = st.capture(2)
+    g.replay()
+    for name, dev in (("Tt", "Tt"), ("state", "psi"), ("slip1", "slip1")):
+        assert np.array_equal(getattr(sim, name), st.get(dev)), name
+    sim.sync_to_host()
+    a = sim.slipv
+    assert a is sim.slipv and np.array_equal(a, st.get("slipv"))
