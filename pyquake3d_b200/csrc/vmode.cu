@@ -74,10 +74,12 @@ __device__ inline void mlp_features(double S, double lk, double a, double b, dou
 }
 
 // 5 -> 64 -> 64 -> 1 tanh network, FP32 (parameters read through the read-only cache).
+// Both loops over the hidden layer are unrolled completely, so the 64 hidden
+// values stay in registers (indexed by constants) instead of local memory.
 __device__ inline float mlp_eval(const float *__restrict__ P, const float *f)
 {
     float h1[MLP_H];
-#pragma unroll 8
+#pragma unroll
     for (int j = 0; j < MLP_H; ++j) {
         float s = __ldg(P + OFF_B1 + j);
 #pragma unroll
@@ -85,11 +87,18 @@ __device__ inline float mlp_eval(const float *__restrict__ P, const float *f)
         h1[j] = tanhf(s);
     }
     float out = __ldg(P + OFF_B3);
-#pragma unroll 2
+#pragma unroll 1
     for (int j = 0; j < MLP_H; ++j) {
         float s = __ldg(P + OFF_B2 + j);
-#pragma unroll 16
-        for (int i = 0; i < MLP_H; ++i) s += __ldg(P + OFF_W2 + MLP_H * j + i) * h1[i];
+        const float4 *w = reinterpret_cast<const float4 *>(P + OFF_W2 + MLP_H * j);
+#pragma unroll
+        for (int i = 0; i < MLP_H / 4; ++i) {
+            const float4 q = __ldg(w + i);
+            s += q.x * h1[4 * i];       // the same products in the same order as a scalar loop
+            s += q.y * h1[4 * i + 1];
+            s += q.z * h1[4 * i + 2];
+            s += q.w * h1[4 * i + 3];
+        }
         out += __ldg(P + OFF_W3 + j) * tanhf(s);
     }
     return out;
