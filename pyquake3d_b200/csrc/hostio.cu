@@ -30,7 +30,9 @@ __global__ void __launch_bounds__(SNAP_THREADS) k_snapshot(SnapFields F, int nf,
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
         const int64_t t = __ldg(iperm + e);
-        for (int j = 0; j < nf; ++j) out[j * n + e] = __ldg(F.f[j] + t);
+#pragma unroll
+        for (int j = 0; j < SNAP_MAX_FIELDS; ++j)      // constant indices: F stays in parameter space
+            if (j < nf) out[j * n + e] = __ldg(F.f[j] + t);
     }
 }
 
