@@ -185,6 +185,26 @@ k_dense_v(const DenseItem *__restrict__ ditems, int64_t n_ditems, const VItem *_
     dense_v_item<TD, TL, TA>(w, ditems, n_ditems, vitems, n_vitems, D, Vd, x, xstride, slots, tpart);
 }
 
+// Sum of the nch chunk partials of one entry of t = V x (stride Q), in chunk
+// order, with four independent loads in flight (a rolled loop waits one L2
+// latency per chunk before a U task can start streaming).
+template <typename TA>
+__device__ __forceinline__ TA sum_partials(const TA *__restrict__ p, int nch, int Q)
+{
+    TA v = 0;
+    int ch = 0;
+    for (; ch + 4 <= nch; ch += 4) {
+        const TA a0 = p[(int64_t)ch * Q], a1 = p[(int64_t)(ch + 1) * Q], a2 = p[(int64_t)(ch + 2) * Q],
+                 a3 = p[(int64_t)(ch + 3) * Q];
+        v += a0;
+        v += a1;
+        v += a2;
+        v += a3;
+    }
+    for (; ch < nch; ++ch) v += p[(int64_t)ch * Q];
+    return v;
+}
+
 // ------------------------------------------------------------------ kernel 2
 // One CTA per (low-rank block, row range): sums the block's chunk partials of
 // t = V x into shared memory, then its warps stream U (lanes over rows).
@@ -225,7 +245,7 @@ __device__ __forceinline__ void u_task(const UTask &T, const TL *__restrict__ U,
         else if (q < T.kS + T.kD) row = 3 * T.kS + c * T.kD + (q - T.kS);
         TA v = 0;
         if (row >= 0)
-            for (int ch = 0; ch < T.nch; ++ch) v += tpart[T.tp + (int64_t)ch * T.Q + row];
+            v = sum_partials<TA>(tpart + T.tp + row, T.nch, T.Q);
         ts[e] = v;
     }
     __syncthreads();
@@ -295,7 +315,7 @@ k_u(const UTask *__restrict__ tasks, const TL *__restrict__ U, const TA *__restr
         else if (q < T.kS + T.kD) row = 3 * T.kS + c * T.kD + (q - T.kS);
         TA v = 0;
         if (row >= 0)
-            for (int ch = 0; ch < T.nch; ++ch) v += tpart[T.tp + (int64_t)ch * T.Q + row];
+            v = sum_partials<TA>(tpart + T.tp + row, T.nch, T.Q);
         ts[e] = v;
     }
     __syncthreads();
