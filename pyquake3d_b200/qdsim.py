@@ -149,6 +149,8 @@ class QDsim:
         self.precision = precision or P.get("Precision", "fp64")
         self.device = device
         self.Init_condition()
+        self.max_slipv1 = float(np.max(np.abs(self.slipv1)))   # updated by every simu_forward
+        self.max_slipv2 = float(np.max(np.abs(self.slipv2)))
         self.tree_block = BlockTree(self, int(P.get("H-matrix leaf size", 32)), float(P.get("Admissibility eta", 2.0)),
                                     int(P.get("Cluster leaf size", 16)))
         self._dev = None
@@ -373,6 +375,9 @@ class QDsim:
         self._reads = set()
         h, dtnext = st.step(dttry, prefetch=tuple(sorted(_STATE[k] for k in reads)))
         self.time = st.time
+        # max |V1|, max |V2| of the step (the values the reference main loop computes
+        # from slipv1 / slipv2 for state.txt), from the step kernel's control block
+        self.max_slipv1, self.max_slipv2 = st.vmax
         return h, dtnext
 
     def snapshot_async(self, names=("slipv", "Tt")):
@@ -561,6 +566,7 @@ class DeviceStepper:
         self.reltol = sim.RelTol
         self.fix_tn = 1 if sim.fix_Tn else 0
         self.time = 0.0
+        self.vmax = (0.0, 0.0)          # max |V1|, max |V2| of the last step()
         self.steps = 0
         self.args = np.zeros(1, dtype=_lib.RK_ARGS)
         for k in self.FIELDS + self.CONST:
@@ -657,6 +663,7 @@ class DeviceStepper:
             raise _lib.Pq3dError(f"time step failed: status {int(c[4])} (h={c[1]:.3e}, rejects={int(c[3])})")
         self.steps += 1
         self.time = float(c[2])
+        self.vmax = (float(c[5]), float(c[6]))
         return float(c[1]), float(c[0])
 
     def _host_io(self):

@@ -139,6 +139,7 @@ def test_reference_loop_reads_current_state(lib, tiny_files):
         m1, m2 = np.max(np.abs(sim.slipv1)), np.max(np.abs(sim.slipv2))
         c = st.ctrl.cpu().numpy()
         assert m1 == c[5] and m2 == c[6], i
+        assert (sim.max_slipv1, sim.max_slipv2) == (m1, m2), i
         for name, dev in (("slipv", "slipv"), ("Tt", "Tt"), ("state", "psi"), ("slip", "slip")):
             assert np.array_equal(getattr(sim, name), st.get(dev)), (i, name)
         slipv_hist.append(sim.slipv)
