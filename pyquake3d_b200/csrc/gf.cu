@@ -243,14 +243,16 @@ PQ3D_EXPORT void TDstressEachSourceAtReceiver_C(double x, double y, double z, co
         fill_nan(strain_out, 6 * n_sources);
         return;
     }
-    for (size_t i = 0; i < n_sources; ++i)
+    for (size_t i = 0; i < n_sources; ++i) {
         for (int k = 0; k < 3; ++k) {
             P9[9 * i + k] = P1_flat[3 * i + k];
             P9[9 * i + 3 + k] = P2_flat[3 * i + k];
             P9[9 * i + 6 + k] = P3_flat[3 * i + k];
-            if (jud_halfspace && (z > 0 || P9[9 * i + 2] > 0 || P9[9 * i + 5] > 0 || P9[9 * i + 8] > 0))
-                printf("Half-space solution: Z coordinates must be negative!\n");
         }
+        // the reference's warning, once per offending source (its TDstressHS runs per source)
+        if (jud_halfspace && (z > 0 || P9[9 * i + 2] > 0 || P9[9 * i + 5] > 0 || P9[9 * i + 8] > 0))
+            printf("Half-space solution: Z coordinates must be negative!\n");
+    }
     int rc = stress_host(&x, &y, &z, 1, P9, n_sources, Ss, Ds, Ts, mu, lambda_, jud_halfspace, stress_out,
                          strain_out);
     free(P9);
