@@ -3,6 +3,9 @@
 // reference's C signatures (src/TDstressFS_C.cpp:2048-2143).
 #include <stdio.h>
 #include <stdlib.h>
+#include <string.h>
+#include <mutex>
+
 #include "pq3d_common.cuh"
 #include "td_gf.cuh"
 #include "td_hs.cuh"
@@ -175,35 +178,95 @@ static void fill_nan(double *a, size_t n)
     for (size_t i = 0; i < n; ++i) a[i] = __builtin_nan("");
 }
 
+// Staging of the drop-ins: per device, one device buffer and one pinned host
+// buffer, grown to the largest call and kept until exit, and one stream.  The
+// reference calls its entry points for every row and column of small blocks,
+// so per-call allocations and several pageable copies would cost more than the
+// work: small calls pack their inputs into the pinned buffer and cross in one
+// copy each way.  Calls on a device are serialised by a mutex (the buffers are
+// shared).
+namespace {
+constexpr int kDropinDevices = 64;
+struct DropinStage {
+    double *buf = nullptr, *hbuf = nullptr;
+    size_t cap = 0, hcap = 0;
+    cudaStream_t st = nullptr;
+};
+std::mutex g_dropin_mu[kDropinDevices];
+DropinStage g_dropin[kDropinDevices];
+
+int grow(double *&p, size_t &cap, size_t need, bool host)
+{
+    if (cap >= need) return PQ3D_OK;
+    const size_t c = need > 2 * cap ? need : 2 * cap;
+    if (p) {
+        if (host) cudaFreeHost(p);
+        else cudaFree(p);
+    }
+    p = nullptr;
+    cap = 0;
+    const cudaError_t e = host ? cudaHostAlloc((void **)&p, c * sizeof(double), cudaHostAllocDefault)
+                               : cudaMalloc((void **)&p, c * sizeof(double));
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return PQ3D_ERR_CUDA;
+    }
+    cap = c;
+    return PQ3D_OK;
+}
+}  // namespace
+
 static int stress_host(const double *X, const double *Y, const double *Z, size_t npt,
                        const double *P9, size_t nsrc, double Ss, double Ds, double Ts, double mu,
                        double lam, bool hs, double *stress, double *strain)
 {
-    size_t np = npt > nsrc ? npt : nsrc;
-    double *dX = nullptr, *dP = nullptr, *dS = nullptr;
-    int rc = PQ3D_OK;
-    if (cudaMalloc(&dX, 3 * npt * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&dP, 9 * nsrc * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&dS, 12 * np * sizeof(double)) != cudaSuccess) {
-        rc = PQ3D_ERR_CUDA;
-    } else {
-        cudaMemcpy(dX, X, npt * sizeof(double), cudaMemcpyHostToDevice);
-        cudaMemcpy(dX + npt, Y, npt * sizeof(double), cudaMemcpyHostToDevice);
-        cudaMemcpy(dX + 2 * npt, Z, npt * sizeof(double), cudaMemcpyHostToDevice);
-        cudaMemcpy(dP, P9, 9 * nsrc * sizeof(double), cudaMemcpyHostToDevice);
-        rc = pq3d_stress_points(dX, dX + npt, dX + 2 * npt, (int64_t)npt, dP, (int64_t)nsrc, Ss, Ds, Ts, mu,
-                                lam, hs ? 2 : 0, dS, dS + 6 * np, 0);
-        if (rc == PQ3D_OK && cudaDeviceSynchronize() != cudaSuccess) rc = PQ3D_ERR_CUDA;
-        if (rc == PQ3D_OK) {
-            if (cudaMemcpy(stress, dS, 6 * np * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) rc = PQ3D_ERR_CUDA;
-            if (strain && cudaMemcpy(strain, dS + 6 * np, 6 * np * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
-                rc = PQ3D_ERR_CUDA;
-        }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDropinDevices) return PQ3D_ERR_CUDA;
+    std::lock_guard<std::mutex> lk(g_dropin_mu[dev]);
+    DropinStage &S = g_dropin[dev];
+    const size_t np = npt > nsrc ? npt : nsrc;
+    const size_t nin = 3 * npt + 9 * nsrc, need = nin + 12 * np;   // inputs, then stress + strain
+    if (!S.st && cudaStreamCreateWithFlags(&S.st, cudaStreamNonBlocking) != cudaSuccess) {
+        S.st = nullptr;
+        return PQ3D_ERR_CUDA;
     }
-    cudaFree(dX);
-    cudaFree(dP);
-    cudaFree(dS);
-    return rc;
+    // small calls: pack into pinned memory, one copy each way; large calls (over
+    // 1 MB) copy the caller's arrays directly, where packing would cost more
+    const bool packed = need * sizeof(double) <= (size_t(1) << 20);
+    if (grow(S.buf, S.cap, need, false) != PQ3D_OK || (packed && grow(S.hbuf, S.hcap, need, true) != PQ3D_OK))
+        return PQ3D_ERR_CUDA;
+    double *h = S.hbuf, *d = S.buf, *dS = d + nin;
+    const cudaStream_t st = S.st;
+    const size_t b = npt * sizeof(double), bp = 9 * nsrc * sizeof(double);
+    if (packed) {
+        memcpy(h, X, b);
+        memcpy(h + npt, Y, b);
+        memcpy(h + 2 * npt, Z, b);
+        memcpy(h + 3 * npt, P9, bp);
+        if (cudaMemcpyAsync(d, h, nin * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess)
+            return PQ3D_ERR_CUDA;
+    } else if (cudaMemcpyAsync(d, X, b, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+               cudaMemcpyAsync(d + npt, Y, b, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+               cudaMemcpyAsync(d + 2 * npt, Z, b, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+               cudaMemcpyAsync(d + 3 * npt, P9, bp, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        return PQ3D_ERR_CUDA;
+    }
+    int rc = pq3d_stress_points(d, d + npt, d + 2 * npt, (int64_t)npt, d + 3 * npt, (int64_t)nsrc, Ss, Ds, Ts, mu,
+                                lam, hs ? 2 : 0, dS, dS + 6 * np, st);
+    if (rc != PQ3D_OK) return rc;
+    const size_t bs = 6 * np * sizeof(double);
+    if (packed) {
+        if (cudaMemcpyAsync(h + nin, dS, (strain ? 2 : 1) * bs, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return PQ3D_ERR_CUDA;
+        memcpy(stress, h + nin, bs);
+        if (strain) memcpy(strain, h + nin + 6 * np, bs);
+        return PQ3D_OK;
+    }
+    if (cudaMemcpyAsync(stress, dS, bs, cudaMemcpyDeviceToHost, st) != cudaSuccess) return PQ3D_ERR_CUDA;
+    if (strain && cudaMemcpyAsync(strain, dS + 6 * np, bs, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return PQ3D_ERR_CUDA;
+    return cudaStreamSynchronize(st) == cudaSuccess ? PQ3D_OK : PQ3D_ERR_CUDA;
 }
 
 // Replaces TDstressFS_C (src/TDstressFS_C.cpp:2048-2095): one source triangle, n receivers.
