@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(ACA_THREADS)
 k_aca(const double *__restrict__ xg, const double *__restrict__ ev, const SrcRec *__restrict__ rec,
       const int32_t *__restrict__ rowlist, const int32_t *__restrict__ collist, const AcaTask *__restrict__ tasks,
       double *__restrict__ ws, double mu, double lam, double eps, int rel_mode, int32_t *__restrict__ rank_out,
-      int32_t *__restrict__ flag_out, const HsRec *__restrict__ hs, int hs_mode)
+      int32_t *__restrict__ flag_out, const HsRec *__restrict__ hs, int hs_mode, int max_mn)
 {
     extern __shared__ uint32_t bits[];
     __shared__ ArgMax red_am[32];
@@ -206,6 +206,13 @@ k_aca(const double *__restrict__ xg, const double *__restrict__ ev, const SrcRec
     __shared__ int s_scan;
 
     const AcaTask T = tasks[blockIdx.x];
+    if (T.m < 0 || T.n < 0 || T.m > max_mn || T.n > max_mn) {   // the pivot bitmaps are sized for max_mn
+        if (threadIdx.x == 0) {
+            rank_out[blockIdx.x] = 0;
+            flag_out[blockIdx.x] = 4;
+        }
+        return;
+    }
     const int m = T.m, n = T.n;
     uint32_t *prevI = bits;
     uint32_t *prevJ = bits + ((m + 31) >> 5);
@@ -404,11 +411,11 @@ PQ3D_EXPORT int pq3d_aca_batched(const double *d_xg, const double *d_ev, const v
         if (hs_mode)
             k_aca<true><<<(unsigned)nt, ACA_THREADS, smem, stream>>>(
                 d_xg, d_ev, (const SrcRec *)d_rec, d_rowlist, d_collist, (const AcaTask *)d_tasks + t0, d_ws, mu,
-                lam, eps, rel_mode, d_rank + t0, d_flags + t0, (const HsRec *)d_hs, hs_mode);
+                lam, eps, rel_mode, d_rank + t0, d_flags + t0, (const HsRec *)d_hs, hs_mode, max_mn);
         else
             k_aca<false><<<(unsigned)nt, ACA_THREADS, smem, stream>>>(
                 d_xg, d_ev, (const SrcRec *)d_rec, d_rowlist, d_collist, (const AcaTask *)d_tasks + t0, d_ws, mu,
-                lam, eps, rel_mode, d_rank + t0, d_flags + t0, nullptr, 0);
+                lam, eps, rel_mode, d_rank + t0, d_flags + t0, nullptr, 0, max_mn);
     }
     return pq3d_launch_status();
 }

@@ -485,6 +485,8 @@ class DeviceHMatrix:
                       "pq3d_aca_batched")
                 ranks = d_rank.cpu().numpy()
                 flags = d_flag.cpu().numpy()
+                if (flags & 4).any():
+                    raise _lib.Pq3dError("pq3d_aca_batched: a task exceeds max_mn (not run)")
                 keep = {}
                 for j, (ti, wo, kmax) in enumerate(batch):
                     if flags[j] & 1 and kmax < min(tasks[ti]["m"], tasks[ti]["n"]):
