@@ -585,6 +585,32 @@ def main():
                    "H-matvec enqueued before the host waits) + slip-rate and traction vectors to pinned "
                    "host memory (QDsim.snapshot_async: gather on a side stream, copy-engine transfer)"}
 
+    # the reference main loop verbatim (src/main.py:161-184): after every step it reads
+    # max |slipv1|, max |slipv2| and keeps the slipv and Tt arrays (device-backed QDsim
+    # attributes, prefetched by the step after the first reads)
+    nl = min(args.steps, 100)
+    _, dttry = sim.simu_forward(dttry)
+    _ = (sim.slipv1, sim.slipv2, sim.slipv, sim.Tt)
+    torch.cuda.synchronize()
+    barrier()
+    kept_v, kept_t = [], []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(nl):
+        h, dtnext = sim.simu_forward(dttry)
+        _ = (np.max(np.abs(sim.slipv1)), np.max(np.abs(sim.slipv2)))
+        kept_v.append(sim.slipv)
+        kept_t.append(sim.Tt)
+        dttry = dtnext
+    e1.record()
+    torch.cuda.synchronize()
+    t_loop = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    e2e["reference_loop"] = {
+        "value": nl * world / t_loop, "unit": "steps/s", "steps": nl,
+        "path": "src/main.py's loop unchanged: simu_forward, np.max(np.abs(slipv1|slipv2)), SLIPV.append(slipv), "
+                "Tt.append(Tt) every step (four 8n-byte vectors to the host per step)"}
+    del kept_v, kept_t
+
     # CPU baseline: the reference's step on the same operator (rank 0, N=1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
