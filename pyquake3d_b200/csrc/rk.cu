@@ -283,8 +283,10 @@ __global__ void __launch_bounds__(RK_THREADS) k_rk_rows_attempt(RkArgs A, int r0
 {
     double e4[4] = {0.0, 0.0, 0.0, 0.0};
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    if (first && A.fuse_rowsum)   // the H-matvec's row sums, staged per CTA (same rows per thread as below)
+        for (int64_t base = r0 + (int64_t)blockIdx.x * RK_THREADS; base < r1; base += stride)
+            rowsum_cta<RK_THREADS>(A, base, r1);
     for (int64_t i = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < r1; i += stride) {
-        if (first && A.fuse_rowsum) fused_rowsum(A, i);
         double e[4];
         dp54_element(A, i, h, e);
 #pragma unroll

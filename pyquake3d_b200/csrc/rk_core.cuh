@@ -59,59 +59,13 @@ constexpr double B81 = 5179. / 57600., B83 = 7571. / 16695., B84 = 393. / 640., 
                  B86 = 187. / 2100., B87 = 1. / 40.;
 
 
-// y[i] = sum of row i's H-matvec slots (the k_rowsum reduction fused into a
-// step kernel); slots are summed in the per-leaf list order.
-template <class A>
-__device__ __forceinline__ void fused_rowsum(const A &S, int64_t i)
-{
-    const int l = S.leaf_of_row[i];
-    double a0 = 0, a1 = 0, a2 = 0;
-    const int k0 = S.leaf_ptr[l], k1 = S.leaf_ptr[l + 1];
-    if (S.slots_fp32) {
-        const float *sl = (const float *)S.slots;
-        int k = k0;
-        for (; k + 4 <= k1; k += 4) {   // four independent loads in flight, list-order sums
-            float v[12];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int64_t s = 3 * ((int64_t)S.leaf_off[k + u] + i);
-                v[3 * u] = sl[s]; v[3 * u + 1] = sl[s + 1]; v[3 * u + 2] = sl[s + 2];
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) { a0 += (double)v[3 * u]; a1 += (double)v[3 * u + 1]; a2 += (double)v[3 * u + 2]; }
-        }
-        for (; k < k1; ++k) {
-            const int64_t s = 3 * ((int64_t)S.leaf_off[k] + i);
-            a0 += (double)sl[s]; a1 += (double)sl[s + 1]; a2 += (double)sl[s + 2];
-        }
-    } else {
-        const double *sl = (const double *)S.slots;
-        int k = k0;
-        for (; k + 4 <= k1; k += 4) {
-            double v[12];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int64_t s = 3 * ((int64_t)S.leaf_off[k + u] + i);
-                v[3 * u] = sl[s]; v[3 * u + 1] = sl[s + 1]; v[3 * u + 2] = sl[s + 2];
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) { a0 += v[3 * u]; a1 += v[3 * u + 1]; a2 += v[3 * u + 2]; }
-        }
-        for (; k < k1; ++k) {
-            const int64_t s = 3 * ((int64_t)S.leaf_off[k] + i);
-            a0 += sl[s]; a1 += sl[s + 1]; a2 += sl[s + 2];
-        }
-    }
-    S.y[3 * i] = a0;
-    S.y[3 * i + 1] = a1;
-    S.y[3 * i + 2] = a2;
-}
-
-// fused_rowsum for the CTA's rows [base, min(base + NT, end)), with all NT
-// threads of the CTA taking part (call from every thread).  The leaf_off range of the CTA's
-// leaves is contiguous (leaves are numbered in row order), so it is staged in
-// shared memory once; then every thread sums its row's slots in list order (the
-// same sums as fused_rowsum) with eight list entries of loads in flight.
+// The H-matvec's row reduction (k_rowsum) fused into the step kernels:
+// y[i] = sum of row i's slots, in the per-leaf list order, for the CTA's rows
+// [base, min(base + NT, end)), with all NT threads of the CTA taking part (call
+// from every thread).  The leaf_off range of the CTA's leaves is contiguous
+// (leaves are numbered in row order), so it is staged in shared memory once;
+// then every thread sums its row's slots with eight list entries of loads in
+// flight.
 constexpr int RS_STAGE = 2048;   // staged leaf_off entries per CTA (larger ranges read them from global)
 
 template <int NT, class A>
