@@ -115,8 +115,9 @@ size_t pq3d_pack_task_bytes(void);
 /* Batched ACA+ (BlockTree.ACA_plus_full_traceS/D, src/Hmatrix.py:581-1011), one
  * CTA per (block, slip pass).  eps: absolute step-size tolerance (rel_mode 0, the
  * reference's 0.01) or relative Frobenius tolerance (rel_mode 1).  Writes the
- * rank and a flag word (1 rank cap reached, 2 B factor all zero, 4 the task is
- * larger than max_mn rows or columns and was not run) per task. */
+ * rank and a flag word (1 rank cap reached, 2 B factor all zero, 4 the pivot
+ * search found every remaining row or column excluded, 8 the task is larger
+ * than max_mn rows or columns and was not run) per task. */
 int pq3d_aca_batched(const double *d_xg, const double *d_ev, const void *d_rec,
                      const int32_t *d_rowlist, const int32_t *d_collist,
                      const void *d_tasks, int64_t n_tasks, double *d_ws, double mu,

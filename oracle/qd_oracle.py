@@ -103,9 +103,20 @@ class Geometry:
         return out
 
 
-def aca_plus(geo, row_cluster, col_cluster, which, eps, iref0, jref0, max_iter=None):
+def aca_plus(geo, row_cluster, col_cluster, which, eps, iref0, jref0, max_iter=None, rel=False):
     """ACA+ of one block for one slip mode; returns dict of U (m x k) and V (k x n)
-    for A1, A2, B (B empty when all its u vectors are zero), and the pivots."""
+    for A1, A2, B (B empty when all its u vectors are zero), and the pivots.
+
+    rel=False: the reference's stop, ||u_k|| ||v_k / alpha|| < eps with eps
+    absolute (src/Hmatrix.py:727,736; eps = 0.01 at :1020-1028).
+    rel=True: the relative stop of the `ACA relative tolerance` key, which has
+    no counterpart in the reference: ||u_k|| ||v_k / alpha|| <= eps ||S_k||_F,
+    where S_k = sum_{p<=k} u_p v_p^T is the A1 approximant after this step and
+    its squared Frobenius norm is updated incrementally,
+        ||S_k||^2 = ||S_{k-1}||^2 + 2 sum_{p<k} (u_p . u_k)(v_p . v_k/alpha)
+                    + ||u_k||^2 ||v_k/alpha||^2,
+    with v_p the stored (pivot-scaled) rows.  Pivots, reference sets and the
+    other stops are the reference's."""
     n_rows, n_cols = len(row_cluster), len(col_cluster)
     us1, vs1, us2, vs2, usB, vsB = [], [], [], [], [], []
     prevI, prevJ = [], []
@@ -171,6 +182,7 @@ def aca_plus(geo, row_cluster, col_cluster, which, eps, iref0, jref0, max_iter=N
     RJstar, RJstar1, RJstar2 = np.zeros(n_rows), np.zeros(n_rows), np.zeros(n_rows)
     RIref, Iref, scan_all = reset_row(iref0)
     RJref, Jref, scan_all = reset_col(jref0)
+    frob2 = 0.0
     for k in range(max_iter):
         mR = np.max(np.abs(RIref), axis=0)
         Jstar = argmax_not_in_list(mR, prevJ)
@@ -200,8 +212,17 @@ def aca_plus(geo, row_cluster, col_cluster, which, eps, iref0, jref0, max_iter=N
         vs2.append(RIstar1.copy() / (alpha1 + 1e-16))
         usB.append(RJstar2.copy())
         vsB.append(np.zeros(len(RIstar2)) if abs(alpha2) < 1e-10 else RIstar2.copy() / (alpha2 + 1e-16))
-        step = np.sqrt(np.sum(u_k ** 2) * np.sum((v_k / alpha) ** 2))
-        if step < eps:
+        su, sv = np.sum(u_k ** 2), np.sum((v_k / alpha) ** 2)
+        step = np.sqrt(su * sv)
+        if rel:
+            w = v_k / alpha
+            cross = 0.0
+            for p in range(len(us1) - 1):
+                cross += np.dot(us1[p], u_k) * np.dot(vs1[p], w)
+            frob2 += 2.0 * cross + su * sv
+            if step <= eps * np.sqrt(abs(frob2)):
+                break
+        elif step < eps:
             break
         if k == max_iter - 1:
             break
@@ -235,7 +256,7 @@ class OracleOperator:
 
     OPS = ("A1s", "A2s", "Bs", "A1d", "A2d", "Bd")
 
-    def __init__(self, geo, blocks, starts=None, eps=0.01):
+    def __init__(self, geo, blocks, starts=None, eps=0.01, rel=False):
         self.geo = geo
         self.blocks = []
         si = 0
@@ -245,8 +266,8 @@ class OracleOperator:
             if aca:
                 (i0, j0), (i1, j1) = starts[si]
                 si += 1
-                S = aca_plus(geo, rc, cc, 1, eps, i0, j0)
-                D = aca_plus(geo, rc, cc, 2, eps, i1, j1)
+                S = aca_plus(geo, rc, cc, 1, eps, i0, j0, rel=rel)
+                D = aca_plus(geo, rc, cc, 2, eps, i1, j1, rel=rel)
                 self.blocks.append(("aca", rc, cc, S, D))
             else:
                 o = geo.gf_block(rc, cc, 3)
@@ -410,3 +431,55 @@ def sim_state(sim):
                 slipv=sim.slipv, slip1=sim.slip1, slip2=sim.slip2, a=sim.a, b=sim.b, dc=sim.dc, f0=sim.f0,
                 shear_loading=sim.shear_loading, normal_loading=sim.normal_loading, slipvC=sim.slipvC,
                 rake0=sim.rake0)
+
+
+# ------------------------------------------------------------------ parallel assembly
+# The reference assembles with an MPI master handing blocks to worker ranks
+# (BlockTree.master / worker / ACA_worker, src/Hmatrix.py:1014-1066, 1136-1260).
+# Here a process pool stands in for the ranks; every block is computed exactly
+# as OracleOperator computes it, and the results are collected in block order.
+_POOL_GEO = {}
+
+
+def _pool_init(geo):
+    _POOL_GEO["geo"] = geo
+
+
+def _pool_block(task):
+    rc, cc, aca, start, eps, rel = task
+    geo = _POOL_GEO["geo"]
+    if aca:
+        (i0, j0), (i1, j1) = start
+        S = aca_plus(geo, rc, cc, 1, eps, i0, j0, rel=rel)
+        D = aca_plus(geo, rc, cc, 2, eps, i1, j1, rel=rel)
+        for d in (S, D):
+            d.pop("prevI", None)
+            d.pop("prevJ", None)
+        return ("aca", rc, cc, S, D)
+    return ("dense", rc, cc, geo.gf_block(rc, cc, 3))
+
+
+def build_operator_parallel(geo, blocks, starts, eps=0.01, rel=False, procs=None):
+    """OracleOperator of `blocks` [(row_cluster, col_cluster, is_aca)] assembled by a
+    pool of `procs` spawned processes (default: every host core).  Largest blocks are
+    handed out first; the block list keeps the input order."""
+    import multiprocessing as mp
+    tasks, si = [], 0
+    for rc, cc, aca in blocks:
+        st = None
+        if aca:
+            st = starts[si]
+            si += 1
+        tasks.append((np.asarray(rc), np.asarray(cc), bool(aca), st, float(eps), bool(rel)))
+    cost = [len(t[0]) * len(t[1]) if not t[2] else 60 * (len(t[0]) + len(t[1])) for t in tasks]
+    order = np.argsort(cost)[::-1]
+    procs = procs or os.cpu_count() or 1
+    out = [None] * len(tasks)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs, initializer=_pool_init, initargs=(geo,)) as pool:
+        for i, res in zip(order, pool.imap(_pool_block, [tasks[i] for i in order], chunksize=4)):
+            out[i] = res
+    op = object.__new__(OracleOperator)
+    op.geo = geo
+    op.blocks = out
+    return op

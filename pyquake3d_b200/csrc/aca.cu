@@ -209,7 +209,7 @@ k_aca(const double *__restrict__ xg, const double *__restrict__ ev, const SrcRec
     if (T.m < 0 || T.n < 0 || T.m > max_mn || T.n > max_mn) {   // the pivot bitmaps are sized for max_mn
         if (threadIdx.x == 0) {
             rank_out[blockIdx.x] = 0;
-            flag_out[blockIdx.x] = 4;
+            flag_out[blockIdx.x] = 8;
         }
         return;
     }

@@ -407,13 +407,23 @@ std::mutex g_scratch_mu;
 double *g_scratch_dev[kMaxDevices] = {nullptr};
 
 // Device address of g_rk_scratch on the current device.  The name is only a
-// host-side stand-in, so the address is looked up once per device (with that
-// device current) and cached.
+// host-side stand-in, so the address is looked up with that device current
+// and cached per device.  Every call checks that the cached address is still
+// device memory of this device: after cudaDeviceReset (or any teardown of the
+// context) the module is loaded again and the address is looked up afresh.
 int scratch_address(double **out)
 {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PQ3D_ERR_CUDA;
     std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (g_scratch_dev[dev]) {
+        cudaPointerAttributes at = {};
+        const cudaError_t e = cudaPointerGetAttributes(&at, g_scratch_dev[dev]);
+        if (e != cudaSuccess || at.type != cudaMemoryTypeDevice || at.device != dev) {
+            (void)cudaGetLastError();   // the failed query must not linger as a sticky launch status
+            g_scratch_dev[dev] = nullptr;
+        }
+    }
     if (!g_scratch_dev[dev]) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_rk_scratch) != cudaSuccess || !p) return PQ3D_ERR_CUDA;

@@ -485,8 +485,11 @@ class DeviceHMatrix:
                       "pq3d_aca_batched")
                 ranks = d_rank.cpu().numpy()
                 flags = d_flag.cpu().numpy()
-                if (flags & 4).any():
-                    raise _lib.Pq3dError("pq3d_aca_batched: a task exceeds max_mn (not run)")
+                if (flags & 8).any():
+                    raise _lib.Pq3dError("pq3d_aca_batched: a task has more rows or columns than the batch's "
+                                         "max_mn (not run)")
+                # flag 4 (every remaining pivot candidate excluded) ends a task normally: the
+                # factors found so far are the block's approximation, as in the reference loop
                 keep = {}
                 for j, (ti, wo, kmax) in enumerate(batch):
                     if flags[j] & 1 and kmax < min(tasks[ti]["m"], tasks[ti]["n"]):

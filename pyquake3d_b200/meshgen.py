@@ -245,8 +245,10 @@ def ensemble_faults(outdir, n_faults=32, seed=4, lo=2000, hi=20000, edge=0.5, pr
     return out
 
 
-def make_case(name, outdir, n_target=None, precision=None):
-    """Write one of the named cases; returns (msh_path, parameter_path)."""
+def make_case(name, outdir, n_target=None, precision=None, tol=None):
+    """Write one of the named cases; returns (msh_path, parameter_path).  n_target
+    resizes `tiny`, `tinynuc`, `thrust20k` (same 100 x 40 km domain, coarser or
+    finer edges) and the curved cases; tol overrides the ACA tolerance."""
     if name == "plain2k":
         P, T = planar(40.0, 20.0, 90.0, 44, 22)
         cols = friction_layout(centroids_km(P, T) * 1e3 / 1e3, 20.0, seed=0)
@@ -270,7 +272,9 @@ def make_case(name, outdir, n_target=None, precision=None):
         return write_case(outdir, name, P, T, cols, leaf=32, tol=0.01, rel=False,
                           precision=precision or "fp64", steps=100)
     if name == "thrust20k":
-        P, T = planar(100.0, 40.0, 30.0, 160, 64, jitter=0.1, seed=1)
+        nz = 64 if n_target is None else max(4, int(round(np.sqrt(n_target / 5.0))))
+        nx = 160 if n_target is None else int(round(2.5 * nz))
+        P, T = planar(100.0, 40.0, 30.0, nx, nz, jitter=0.1, seed=1)
         xc = centroids_km(P, T)
         dd = -xc[:, 2] / np.sin(np.deg2rad(30.0))   # down-dip distance
         patch = lambda c: (np.abs(c[:, 0]) <= 30.0) & (np.abs(-c[:, 2] / np.sin(np.deg2rad(30.0)) - 20.0) <= 10.0)
@@ -278,7 +282,7 @@ def make_case(name, outdir, n_target=None, precision=None):
                                nuc=((-20.0e0, 20.0 * np.cos(np.deg2rad(30.0)), -10.0), 3.0, 1e-6))
         cols[:, 0] = np.pi / 2   # thrust: rake 90 degrees
         del dd
-        return write_case(outdir, name, P, T, cols, leaf=64, tol=1e-4, rel=True,
+        return write_case(outdir, name, P, T, cols, leaf=64, tol=tol or 1e-4, rel=True,
                           precision=precision or "fp32", steps=20000)
     if name in ("curved60k", "curved120k"):
         n = n_target or (60000 if name == "curved60k" else 120000)
@@ -289,6 +293,6 @@ def make_case(name, outdir, n_target=None, precision=None):
             amb = gaussian_field(xc, 5.0, seed=3, lo=-0.006, hi=0.006)
             cols[:, 1] = cols[:, 2] + amb
             cols[:, 6] = gaussian_field(xc, 5.0, seed=4, lo=20.0, hi=80.0)
-        return write_case(outdir, name, P, T, cols, leaf=64, tol=1e-5, rel=True,
+        return write_case(outdir, name, P, T, cols, leaf=64, tol=tol or 1e-5, rel=True,
                           precision=precision or "bf16", steps=20000 if name == "curved60k" else 50000)
     raise ValueError(name)

@@ -1,8 +1,10 @@
 """Generate the golden fixtures in tests/golden/ by running the REFERENCE itself.
 
-Run in a container that has the reference tree (default /root/reference):
+Run in a container that has the reference tree: the --ref argument, else the
+PQ3D_REFERENCE environment variable, else a tree named `reference` beside this
+repository's checkout:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref <reference tree>]
 
 What it does:
   * builds the reference's TDstressFS_C.cpp from source (oracle/Makefile, target
@@ -410,7 +412,8 @@ def tiny_hs_case(work, QDsim_mod, readmsh):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PQ3D_REFERENCE") or
+                    os.path.abspath(os.path.join(REPO, os.pardir, "reference")))
     ap.add_argument("--only", default=None, help="regenerate one fixture: gf | tiny | hs | tiny_hs | output")
     args = ap.parse_args()
     ref_src = os.path.join(args.ref, "src")
