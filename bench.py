@@ -161,35 +161,60 @@ def export_host_operator(op):
     return ho
 
 
-def cpu_reference_steps(ho, state, V0, mu, Cs, budget_s, max_steps=20):
-    """The reference's step (oracle port) on the host: returns (steps/s, steps, seconds)."""
+def cpu_reference_steps(ho, state, V0, mu, Cs, budget_s, max_steps=20, dttry=1e-3, reltol=1e-4, fix_tn=False):
+    """The reference's step (oracle port) on the host: returns (steps/s, steps, seconds,
+    the oracle stepper, its accepted step sizes)."""
     import qd_oracle
-    st = qd_oracle.OracleStepper(state, qd_oracle.operator_mvm(ho), V0, mu, Cs)
-    dttry = 1e-3
+    st = qd_oracle.OracleStepper(state, qd_oracle.operator_mvm(ho), V0, mu, Cs, reltol, fix_tn)
     t0 = time.perf_counter()
     k = 0
+    hs = []
     while k < max_steps:
-        _, dttry = st.simu_forward(dttry)
+        h, dttry = st.simu_forward(dttry)
+        hs.append(h)
         k += 1
         if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
-    return k / dt, k, dt
+    return k / dt, k, dt, st, hs
+
+
+def pin_fp64_to_oracle(sim, op, ost, hs):
+    """The device FP64 stepper from the same initial state, stepped adaptively as
+    many steps as the oracle took: relative differences of h and of the state."""
+    from pyquake3d_b200.qdsim import DeviceStepper
+    d = DeviceStepper(sim, op, "fp64")
+    dt = sim.htry
+    hd = []
+    for _ in hs:
+        h, dt = d.step(dt)
+        hd.append(h)
+    out = {"steps": len(hs), "h_max_rel_diff": float(np.max(np.abs(np.array(hd) - hs) / np.array(hs)))}
+    for name, dev in (("slip1", "slip1"), ("state", "psi"), ("Tt1o", "Tt1o"), ("Tno", "Tno"), ("slipv", "slipv")):
+        r = getattr(ost, name)
+        out[name + "_max_rel_diff"] = float(np.abs(d.get(dev) - r).max() / np.abs(r).max())
+    return out
 
 
 def accuracy_study(sim, op, nrep, precisions=("bf16",), marks=(50, 100, 200, 500)):
-    """Relative L2 errors of slip, V and psi of each precision against the FP64 operator
-    at equal times (dt replay of the FP64 run), after each mark; plus the FP64 chaos
-    floor: the same errors between two FP64 runs whose initial shear tractions differ by a
-    relative 1e-12."""
+    """Relative L2 errors of slip, V, psi and theta of each precision against the FP64
+    operator at equal times (dt replay of the FP64 run), after each mark; plus the FP64
+    chaos floor: the same errors between two FP64 runs whose initial shear tractions
+    differ by a relative 1e-12.  The FP64 device path itself is pinned to the oracle's
+    simu_forward on the same operator (the cpu_baseline leg and the GPU tests)."""
     import torch
     from pyquake3d_b200.qdsim import DeviceStepper
+
+    def theta(st):
+        # state variable theta = (Dc / V0) exp((psi - f0) / b) of the log-state psi
+        return st.t["dc"] / st.V0 * torch.exp((st.t["psi"] - st.t["f0"]) / st.t["b"])
 
     def errs(a, b):
         sa = torch.sqrt(a.t["slip1"] ** 2 + a.t["slip2"] ** 2)
         sb = torch.sqrt(b.t["slip1"] ** 2 + b.t["slip2"] ** 2)
         r = lambda u, v: float(torch.linalg.norm(u - v) / torch.linalg.norm(v))
-        return {"slip": r(sa, sb), "V": r(a.t["slipv"], b.t["slipv"]), "psi": r(a.t["psi"], b.t["psi"])}
+        return {"slip": r(sa, sb), "V": r(a.t["slipv"], b.t["slipv"]), "psi": r(a.t["psi"], b.t["psi"]),
+                "theta": r(theta(a), theta(b))}
 
     marks = [m for m in marks if m <= nrep] or [nrep]
     ref = DeviceStepper(sim, op, "fp64")
@@ -343,11 +368,18 @@ def ensemble_study(nsteps, nrep, faults=32):
     return out
 
 
-def _worker_init(blocks):
-    _W["blocks"] = blocks
+def _rank_init(geo, tasks, oracle_dir):
+    """One emulated MPI rank of the reference: assemble its share of the blocks (as
+    ACA_worker does on every rank, src/Hmatrix.py:1014-1066) and keep them."""
+    if oracle_dir not in sys.path:
+        sys.path.insert(0, oracle_dir)
+    import qd_oracle
+    qd_oracle._pool_init(geo)
+    _W["blocks"] = [qd_oracle._pool_block(t) for t in tasks]
 
 
-def _worker_mvm(args):
+def _rank_mvm(args):
+    """This rank's part of the six products (blocks_process_MVM on its local blocks)."""
     import qd_oracle
     x1, x2 = args
     ho = object.__new__(qd_oracle.OracleOperator)
@@ -355,55 +387,100 @@ def _worker_mvm(args):
     return qd_oracle.operator_mvm(ho)(x1, x2)
 
 
+def _rank_ready(_):
+    return len(_W["blocks"])
+
+
+def _maps_with(name):
+    try:
+        return sorted({l.split()[-1] for l in open("/proc/self/maps") if name in l and l.split()[-1].startswith("/")})
+    except OSError:
+        return []
+
+
 def run_reference(args, rank, world):
+    """The reference's CPU path on the host cores, on the GPU arm's workload and step
+    counts.  Nothing of the product's compute path is loaded here: the mesh and the
+    initial state come from the host-only input modules (pure numpy restatements of
+    read_mshV2 / Init_condition, pinned bitwise to the reference), the operator is
+    assembled on the CPU by the oracle (C Green's function + numpy ACA+, relative
+    tolerance 1e-5 as in the workload) in worker processes that emulate the
+    reference's MPI ranks -- each assembles and keeps its share of the blocks, as
+    ACA_worker does -- and every step runs the oracle's simu_forward with the six
+    block-loop MVMs split over those ranks and summed (the reference's
+    reduce(SUM), src/QDsim.py:906-922)."""
     if rank != 0:
         print(json.dumps({"impl": "reference", "rank": rank, "skipped": "rank 0 runs the CPU arm"}), file=sys.stderr)
         return
     import multiprocessing as mp
-    import torch
     import qd_oracle
     from pyquake3d_b200 import QDsim, read_mshV2
+    from pyquake3d_b200.hmatrix import aca_start_indices
+    t0 = time.perf_counter()
     msh, para = make_case(rank)
     nodes, tris = read_mshV2(msh)
-    sim = QDsim(tris, nodes, para, device="cuda:0", precision="fp64")
-    # The operator values are produced on the device (CPU assembly at this size takes
-    # about an hour) and copied to the host; everything timed below runs on the CPU.
-    ho = export_host_operator(sim.tree_block.op())
-    del sim.tree_block._op
-    torch.cuda.empty_cache()
+    sim = QDsim(tris, nodes, para, device="cpu", precision="fp64")
+    st = sim.tree_block.struct
+    tol = float(sim.Para0.get("ACA tolerance", 0.01))
+    rel = sim.Para0.get("ACA relative tolerance", "False") == "True"
+    starts = aca_start_indices(st.blocks, int(sim.Para0.get("ACA seed", 0)))
+    geo = qd_oracle.Geometry(sim.xg, sim.eleVec, sim.nodelst, sim.elelst, sim.mu, sim.lambda_)
+    tasks, si = [], 0
+    for b in st.blocks:
+        s0 = None
+        if b.aca:
+            s0 = starts[si]
+            si += 1
+        tasks.append((np.asarray(b.row.indices), np.asarray(b.col.indices), bool(b.aca), s0, tol, rel))
     cores = os.cpu_count() or 1
-    nproc = max(1, min(cores, 32))
-    chunks = [ho.blocks[i::nproc] for i in range(nproc)]
+    nproc = max(1, min(cores, 64))
+    # balance the ranks by assembly cost (largest first, to the least loaded rank)
+    cost = [len(t[0]) * len(t[1]) if not t[2] else 60 * (len(t[0]) + len(t[1])) for t in tasks]
+    share, load = [[] for _ in range(nproc)], np.zeros(nproc)
+    for i in np.argsort(cost)[::-1]:
+        r = int(np.argmin(load))
+        share[r].append(tasks[i])
+        load[r] += cost[i]
     ctx = mp.get_context("spawn")
-    pools = [ctx.Pool(1, initializer=_worker_init, initargs=(c,)) for c in chunks]
+    odir = os.path.join(REPO, "oracle")
+    pools = [ctx.Pool(1, initializer=_rank_init, initargs=(geo, share[r], odir)) for r in range(nproc)]
+    nblk = sum(p.apply(_rank_ready, (0,)) for p in pools)
+    assert nblk == len(tasks)
+    t_asm = time.perf_counter() - t0
 
     def mvm(x1, x2):
-        res = [p.apply_async(_worker_mvm, ((x1, x2),)) for p in pools]
+        res = [p.apply_async(_rank_mvm, ((x1, x2),)) for p in pools]
         parts = [r.get() for r in res]
         return tuple(sum(p[k] for p in parts) for k in range(3))   # the reference's reduce(SUM)
 
-    st = qd_oracle.OracleStepper(qd_oracle.sim_state(sim), mvm, sim.V0, sim.mu, sim.Cs)
+    ost = qd_oracle.OracleStepper(qd_oracle.sim_state(sim), mvm, sim.V0, sim.mu, sim.Cs, sim.RelTol, sim.fix_Tn)
     dttry = sim.htry
-    nwarm = min(args.warmup, 3)              # args.warmup is at least 3
+    # the GPU arm's step counts; larger requests are capped so the arm ends in minutes
+    nwarm = min(args.warmup, 20)
+    nsteps = max(1, min(args.steps, 200))
     for _ in range(nwarm):
-        _, dttry = st.simu_forward(dttry)
-    nsteps = max(1, min(args.steps, 10))
-    t0 = time.perf_counter()
+        _, dttry = ost.simu_forward(dttry)
+    t1 = time.perf_counter()
     for _ in range(nsteps):
-        _, dttry = st.simu_forward(dttry)
-    dt = time.perf_counter() - t0
+        _, dttry = ost.simu_forward(dttry)
+    dt = time.perf_counter() - t1
     for p in pools:
         p.close()
     v = nsteps / dt
     line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "steps/s", "n_gpus": world,
             "steps": nsteps, "warmup": nwarm, "ms_per_step": 1e3 * dt / nsteps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": CASE + " (59,696 triangles, H-matrix leaf 64, eta 2, ACA rel 1e-5)",
-                       "path": "reference CPU step: six block-loop MVMs (MPI block split emulated by %d worker "
-                               "processes + sum) and DP5(4) in numpy, FP64" % nproc},
+            "config": {"workload": CASE + " (%d triangles, H-matrix leaf %d, eta 2, ACA %s %g)" % (
+                           st.n, st.mini_leaf, "relative" if rel else "absolute", tol),
+                       "path": "reference CPU path: operator assembled on the CPU (C Green's function, numpy ACA+) "
+                               "by %d processes emulating the MPI ranks, each keeping its blocks; per step the six "
+                               "block-loop MVMs on every rank + sum and DP5(4), numpy FP64" % nproc,
+                       "assembly_s": round(t_asm, 1),
+                       "steps_requested": args.steps, "warmup_requested": args.warmup},
             "cpu_baseline": {"value": v, "unit": "steps/s", "cores": nproc, "kind": "port",
-                             "sample": "%d steps of the 60k case after warm-up" % nsteps},
-            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                             "sample": "%d steps of the %d-triangle case after %d warm-up steps" % (nsteps, st.n, nwarm)},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "repo_libraries_loaded": [m for m in _maps_with(".so") if m.startswith(REPO)]}
     print(json.dumps(line))
 
 
@@ -421,27 +498,30 @@ def main():
     ap.add_argument("--vmode-steps", type=int, default=60)
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 32-fault ensemble study")
     ap.add_argument("--ensemble-steps", type=int, default=500)
+    ap.add_argument("--accuracy-steps", type=int, default=500,
+                    help="horizon of the error study against the FP64 path (dt replay)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp64"],
                     help="operator storage of the headline path (fp32: meets the 1e-5 slip target)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     set_case(args.case)
 
-    import torch
-    import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        # CPU only: rank 0 runs the reference's path on the host cores, the other ranks
+        # exit at once (no process group, no CUDA context)
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     torch.cuda.set_device(local)
-    if args.impl == "reference":
-        run_reference(args, rank, world)
-        if world > 1:
-            dist.destroy_process_group()
-        return
 
     # batched ensemble of 32 independent faults (one launch per step for all); run first,
     # on an empty device: its ACA workspaces (all live until packing) are the run's peak
@@ -550,7 +630,8 @@ def main():
     gf = gf_roofline(op, sim.tree_block.struct)
 
     # accuracy vs the FP64 path at equal times (dt replay of the FP64 run), at several horizons
-    accuracy = accuracy_study(sim, op, min(args.steps, 500), precisions=("bf16", "fp32"))
+    # (a fixed horizon, independent of the timed step count)
+    accuracy = accuracy_study(sim, op, args.accuracy_steps, precisions=("bf16", "fp32"))
 
     # V-mode: DP5(4) with one H-matvec per stage and a Newton solve for V; MLP seed
     # trained on the run's own solves (hand-written kernels)
@@ -613,17 +694,21 @@ def main():
 
     # CPU baseline: the reference's step on the same operator (rank 0, N=1)
     cpu = None
+    pinned = None
     if rank == 0 and world == 1 and not args.no_cpu:
         import qd_oracle
         from pyquake3d_b200 import QDsim as Q2
         ho = export_host_operator(op)
         host = Q2(tris, nodes, para, device="cuda:0", precision="bf16")
-        crate, k, secs = cpu_reference_steps(ho, qd_oracle.sim_state(host), host.V0, host.mu, host.Cs,
-                                             args.cpu_budget)
+        crate, k, secs, ost, hs = cpu_reference_steps(ho, qd_oracle.sim_state(host), host.V0, host.mu, host.Cs,
+                                                      args.cpu_budget, dttry=host.htry, reltol=host.RelTol,
+                                                      fix_tn=host.fix_Tn)
         cpu = {"value": crate, "unit": "steps/s", "cores": 1, "kind": "port",
                "sample": "%d steps (%.1f s) of the same 60k workload: six block-loop MVMs + DP5(4), "
                          "numpy FP64, one process" % (k, secs)}
         del ho
+        # the device FP64 path pinned to the oracle over those steps (same operator)
+        pinned = pin_fp64_to_oracle(host, op, ost, hs)
 
     traffic = None
     tp = os.path.join(REPO, "profiles", "hmatvec_traffic.json")
@@ -654,12 +739,14 @@ def main():
                      "kernel": "H-matvec (k_v + k_du), " + prec_text[head].split(",")[0],
                      "alg_bytes": mv[head]["alg_bytes"], "ms": mv[head]["ms"], "peak_source": peak_kind},
         "slip_rel_err_vs_fp64": err_head.get("slip"),
+        "err_vs_fp64_at_horizon": dict(err_head, horizon_steps=args.accuracy_steps) if err_head else None,
         "plain_fp64": {"steps_per_s": rate["fp64"], "ms_per_step": 1e3 * timing["fp64"] / args.steps,
                        "hmatvec": mv["fp64"]},
         "mixed_vs_plain": rate[head] / rate["fp64"],
         "all_precisions": {p: {"steps_per_s": rate[p], "ms_per_step": 1e3 * timing[p] / args.steps,
                                "hmatvec": mv[p], "vs_fp64": rate[p] / rate["fp64"]} for p in steppers},
         "accuracy_vs_fp64": accuracy,
+        "fp64_pinned_to_oracle": pinned,
         "vmode": vmode,
         "ensemble": ensemble,
         "gf_assembly": gf,

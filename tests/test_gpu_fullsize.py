@@ -15,6 +15,10 @@ sizes the product is checked by properties that hold at any size:
   fused single-GPU step at the 20k thrust workload;
 * plain2k (one dense FP64 block) is small enough for the oracle itself: its
   operator rows and 50 adaptive steps against the oracle on the same operator;
+* curved60k and thrust20k: the device-assembled FP64 operator copied to the
+  host drives the oracle's simu_forward for 12 adaptive steps beside the device
+  FP64 stepper (h and state pinned to the oracle) and the FP32-operator stepper
+  on the oracle's step sizes (slip, V and theta within the 1e-5 target);
 * curved120k in V-mode: the MLP-seeded and the undamped-start runs agree.
 
 Workloads: plain2k (1,936 triangles, vertical strike-slip), thrust20k (20,480
@@ -229,3 +233,69 @@ def test_vmode_curved120k_mlp_seed_matches_newton(lib, tmp_path_factory):
     assert np.linalg.norm(runs[2][1] - runs[1][1]) <= 1e-9 * np.linalg.norm(runs[1][1])
     s = runs[2][2]
     assert s["fallbacks"] <= 0.01 * s["solves"], s
+
+
+def _theta(psi, dc, f0, b, V0):
+    """State variable theta = (Dc / V0) exp((psi - f0) / b) of the log-state psi."""
+    return dc / V0 * np.exp((psi - f0) / b)
+
+
+def _pin_to_oracle(sim, op, nsteps=12):
+    """Device FP64 and FP32 steppers against the oracle's simu_forward on the device's
+    own FP64 operator copied to the host (the operator the reference path would
+    apply, pinned blockwise by the parity tests).  Returns the worst errors."""
+    import qd_oracle
+    from pyquake3d_b200.hmatrix import export_blocks
+    from pyquake3d_b200.qdsim import DeviceStepper
+    ho = object.__new__(qd_oracle.OracleOperator)
+    ho.blocks = export_blocks(op)
+    ost = qd_oracle.OracleStepper(qd_oracle.sim_state(sim), qd_oracle.operator_mvm(ho), sim.V0, sim.mu, sim.Cs,
+                                  sim.RelTol, sim.fix_Tn)
+    d64 = DeviceStepper(sim, op, "fp64")
+    dt_o = dt_d = sim.htry
+    hs = []
+    for i in range(nsteps):
+        h_o, dt_o = ost.simu_forward(dt_o)
+        h_d, dt_d = d64.step(dt_d)
+        assert abs(h_d - h_o) <= 1e-9 * abs(h_o), (i, h_d, h_o)
+        hs.append(h_o)
+    del ho
+    out = {}
+    for name, dev in (("slip1", "slip1"), ("slip2", "slip2"), ("state", "psi"), ("Tno", "Tno"), ("Tt1o", "Tt1o"),
+                      ("slipv", "slipv")):
+        r = getattr(ost, name)
+        out["fp64_" + name] = float(np.abs(d64.get(dev) - r).max() / np.abs(r).max())
+    # FP32 operator on the oracle's step sizes
+    d32 = DeviceStepper(sim, op, "fp32")
+    d32.set_replay(torch.tensor(hs, dtype=torch.float64, device="cuda"))
+    d32.run(nsteps, sim.htry)
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    slip_o = np.sqrt(ost.slip1 ** 2 + ost.slip2 ** 2)
+    out["fp32_slip"] = rel(np.sqrt(d32.get("slip1") ** 2 + d32.get("slip2") ** 2), slip_o)
+    out["fp32_V"] = rel(d32.get("slipv"), ost.slipv)
+    th_o = _theta(ost.state, ost.dc, ost.f0, ost.b, sim.V0)
+    out["fp32_theta"] = rel(_theta(d32.get("psi"), ost.dc, ost.f0, ost.b, sim.V0), th_o)
+    return out
+
+
+def test_curved60k_pinned_to_oracle(c60):
+    """curved60k: 12 adaptive steps of the oracle's simu_forward on the device's FP64
+    operator (copied to the host) beside the device FP64 stepper (h to 1e-9, state
+    to 1e-8) and the FP32-operator stepper on the oracle's step sizes (slip, V and
+    theta relative L2 within the 1e-5 target)."""
+    sim, op = c60
+    e = _pin_to_oracle(sim, op)
+    for k, v in e.items():
+        lim = 1e-8 if k.startswith("fp64") else 1e-5
+        assert v <= lim, (k, v, e)
+
+
+def test_thrust20k_pinned_to_oracle(lib, tmp_path_factory):
+    """thrust20k (20,480 triangles, ACA relative 1e-4): the same pin as curved60k."""
+    sim = _case("thrust20k", tmp_path_factory, "fp32")
+    sim.tree_block.want = ("fp64", "fp32")
+    op = sim.tree_block.op()
+    e = _pin_to_oracle(sim, op)
+    for k, v in e.items():
+        lim = 1e-8 if k.startswith("fp64") else 1e-5
+        assert v <= lim, (k, v, e)
