@@ -500,7 +500,7 @@ def main():
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--accuracy-steps", type=int, default=500,
                     help="horizon of the error study against the FP64 path (dt replay)")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp64"],
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp64", "mixed"],
                     help="operator storage of the headline path (fp32: meets the 1e-5 slip target)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -538,13 +538,13 @@ def main():
     nodes, tris = read_mshV2(msh)
     t0 = time.perf_counter()
     sim = QDsim(tris, nodes, para, device="cuda:%d" % local, precision=args.precision)
-    sim.tree_block.want = ("fp64", "bf16", "fp32")
+    sim.tree_block.want = ("fp64", "bf16", "fp32", "mixed")
     t_host = time.perf_counter() - t0
     op = sim.tree_block.op()
     t_asm = time.perf_counter() - t0 - t_host
     kS, kD = op.ranks()
     head = args.precision
-    steppers = {p: DeviceStepper(sim, op, p) for p in ("fp32", "bf16", "fp64")}
+    steppers = {p: DeviceStepper(sim, op, p) for p in ("fp32", "bf16", "fp64", "mixed")}
     plans = {p: op.plan(p) for p in steppers}
 
     def barrier():
@@ -631,7 +631,7 @@ def main():
 
     # accuracy vs the FP64 path at equal times (dt replay of the FP64 run), at several horizons
     # (a fixed horizon, independent of the timed step count)
-    accuracy = accuracy_study(sim, op, args.accuracy_steps, precisions=("bf16", "fp32"))
+    accuracy = accuracy_study(sim, op, args.accuracy_steps, precisions=("bf16", "fp32", "mixed"))
 
     # V-mode: DP5(4) with one H-matvec per stage and a Newton solve for V; MLP seed
     # trained on the run's own solves (hand-written kernels)
@@ -720,13 +720,15 @@ def main():
     nlaunch_step = (2 if plans[head]["n_utasks"] > 0 else 1) + 1
     prec_text = {"fp32": "fp32 operator (near field + low rank), fp64 state and slip",
                  "bf16": "bf16 low rank / fp32 near field, fp64 state and slip",
-                 "fp64": "fp64 operator and state"}
+                 "fp64": "fp64 operator and state",
+                 "mixed": "fp32 near field / low-rank terms in fp32, fp16 or int8 by weight, fp64 state and slip"}
     err_head = accuracy.get(head, [{}])[-1] if head in accuracy else {}
     line = {
         "metric": METRIC, "value": rate[head], "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * timing[head] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": {"fp32": "f32 operator, f64 state", "bf16": "bf16+f32 operator, f64 state", "fp64": "f64"}[head],
+        "dtype": {"fp32": "f32 operator, f64 state", "bf16": "bf16+f32 operator, f64 state", "fp64": "f64",
+                  "mixed": "f32+f16+i8 operator, f32 accumulation, f64 state"}[head],
         "data": "synthetic",
         "config": {"workload": CASE + " (%d triangles)" % sim.xg.shape[0], "precision": prec_text[head],
                    "leaf": int(sim.tree_block.mini_leaf), "eta": 2.0, "aca": "relative 1e-5",
@@ -745,6 +747,9 @@ def main():
         "mixed_vs_plain": rate[head] / rate["fp64"],
         "all_precisions": {p: {"steps_per_s": rate[p], "ms_per_step": 1e3 * timing[p] / args.steps,
                                "hmatvec": mv[p], "vs_fp64": rate[p] / rate["fp64"]} for p in steppers},
+        "mixed_storage": {"tolerance": plans["mixed"]["mixed"]["tol"],
+                          "terms_fp32_fp16_int8": [int(sum(c)) for c in plans["mixed"]["mixed"]["class_terms"]],
+                          "stored_bytes": int(plans["mixed"]["stored_bytes"])},
         "accuracy_vs_fp64": accuracy,
         "fp64_pinned_to_oracle": pinned,
         "vmode": vmode,

@@ -129,16 +129,41 @@ int pq3d_aca_pack(const void *d_tasks, int64_t n_tasks, const double *d_ws,
                   const int32_t *d_rowlist, const int32_t *d_collist, const int32_t *d_iperm,
                   int dtype, void *d_U, void *d_V, cudaStream_t stream);
 
+/* Mixed storage of the low-rank factors (storage code 3 of pq3d_hmatvec; no
+ * counterpart in the reference, which applies every block in FP64,
+ * src/Hmatrix.py:1445-1538).  Each ACA term u v^T is stored as FP32, FP16 or
+ * INT8 according to its weight w = max_i(|u_i| / R_i) * ||v||_1, R_i the
+ * near-field absolute row sum of row i (largest component): the size of the
+ * row error a quantised term can cause, against the scale at which FP32
+ * storage of the row already rounds.
+ *  pq3d_nearfield_rowabs: R3[c * n + i] += sum over dense blocks of |K^c_ij|
+ *    (both slips); d_blocks are the DenseBlock records (off32 used), R3 zeroed.
+ *  pq3d_aca_term_weights: w per (task, term) into d_w[tmap_off + q].
+ *  pq3d_aca_pack_mixed: the factors in the class arrays (zeroed beforehand) and
+ *    the FP16 / INT8 per-V-row scales.  Task records: pq3d_pack_mixed_task_bytes(). */
+size_t pq3d_pack_mixed_task_bytes(void);
+int pq3d_nearfield_rowabs(const float *d_dense32, const void *d_blocks, int64_t n_blocks, int n, double *d_R3,
+                          cudaStream_t stream);
+int pq3d_aca_term_weights(const void *d_tasks, int64_t n_tasks, const double *d_ws, const int32_t *d_rowlist,
+                          const int32_t *d_iperm, const double *d_R, double *d_w, cudaStream_t stream);
+int pq3d_aca_pack_mixed(const void *d_tasks, int64_t n_tasks, const double *d_ws, const int32_t *d_rowlist,
+                        const int32_t *d_collist, const int32_t *d_iperm, const int32_t *d_tmap, float *d_U32,
+                        void *d_U16, void *d_U8, float *d_V32, void *d_V16, void *d_V8, float *d_scales,
+                        cudaStream_t stream);
+
 /* ---------------------------------------------------------------- H-matvec */
 
 /* Sizes of the work-item records: kind 0 DenseItem, 1 VItem, 2 UTask,
- * 4 DenseBlock, 5 the plan struct. */
+ * 4 DenseBlock, 5 the plan struct, 6 the mixed-storage U task. */
 size_t pq3d_item_bytes(int kind);
 
 /* y (n x 3, FP64) = [A1s A1d; A2s A2d; Bs Bd] x (+ add0/add1/add2 per component).
  * Replaces the six BlockTree.blocks_process_MVM calls of QDsim.simu_forward
  * (src/Hmatrix.py:1445-1538, src/QDsim.py:906-917).  plan_host is a host copy of
- * the plan (device pointers inside); x interleaved strike/dip deficit.  d_y may be
+ * the plan (device pointers inside); x interleaved strike/dip deficit.  Plan
+ * dtype: 0 FP64, 1 FP32, 2 FP32 dense + BF16 low rank, 3 FP32 dense + mixed low
+ * rank (FP32 / FP16 / INT8 term classes, the class arrays and scales in the
+ * plan's trailing fields).  d_y may be
  * NULL: then only the per-row partial sums (d_slots) are written, for the step
  * kernel to reduce. */
 int pq3d_hmatvec(const void *plan_host, const void *d_x, void *d_slots, void *d_tpart,

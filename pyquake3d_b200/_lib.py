@@ -28,7 +28,15 @@ PACK_TASK = np.dtype([("ws_off", "i8"), ("u_off", "i8"), ("v_off", "i8"), ("rows
 _PLAN_PTRS = ["dense", "U", "V", "ditems", "vitems", "utasks", "leaf_of_row", "leaf_ptr", "leaf_off"]
 HM_PLAN = np.dtype([("n", "i4"), ("dtype", "i4")] + [(p, "u8") for p in _PLAN_PTRS] +
                    [(k, "i8") for k in ("n_ditems", "n_vitems", "n_utasks", "n_slots", "n_tpart")] +
-                   [("kmax", "i4"), ("pad", "i4")], align=True)
+                   [("kmax", "i4"), ("pad", "i4")] +
+                   [(p, "u8") for p in ("U16", "V16", "U8", "V8", "scales")], align=True)
+# mixed storage (FP32 / FP16 / INT8 term classes): U task and packing records
+U_TASK_M = np.dtype([("off", "i8", 3), ("m", "i4"), ("r0", "i4"), ("r1", "i4"), ("slot", "i4")] +
+                    [(k, "i4", 3) for k in ("K", "kS", "kD", "Q", "tp", "nch", "sb")] + [("pad", "i4")], align=True)
+PACK_TASK_M = np.dtype([("ws_off", "i8"), ("rows_off", "i8"), ("cols_off", "i8"), ("tmap_off", "i8"),
+                        ("u_off", "i8", 3), ("v_off", "i8", 3)] +
+                       [(k, "i4") for k in ("m", "n", "kmax", "k", "pass_", "r0", "c0", "zeroB")] +
+                       [(k, "i4", 3) for k in ("kS", "kD", "Q", "K", "sb")] + [("pad", "i4")], align=True)
 _RK_PTRS = ["Tno", "Tt1o", "Tt2o", "psi", "slip1", "slip2", "slipv1", "slipv2", "slipv", "rake", "Tt", "fric", "slip",
             "a", "b", "dc", "f0", "shear_loading", "normal_loading", "vplc", "cr0", "sr0",
             "y", "cand", "blk", "x", "ctrl", "hist", "hforce", "bar", "slots", "leaf_of_row", "leaf_ptr", "leaf_off",
@@ -97,6 +105,10 @@ def load():
     L.pq3d_item_bytes.argtypes = [i32]
     L.pq3d_item_bytes.restype = ctypes.c_size_t
     L.pq3d_hmatvec.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.pq3d_pack_mixed_task_bytes.restype = ctypes.c_size_t
+    L.pq3d_nearfield_rowabs.argtypes = [vp, vp, i64, i32, vp, vp]
+    L.pq3d_aca_term_weights.argtypes = [vp, i64, vp, vp, vp, vp, vp, vp]
+    L.pq3d_aca_pack_mixed.argtypes = [vp, i64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.pq3d_rk_args_bytes.restype = ctypes.c_size_t
     L.pq3d_rk_grid.argtypes = [i32]
     L.pq3d_rk_step.argtypes = [vp, i32, vp]
@@ -114,13 +126,15 @@ def load():
     L.pq3d_ens_grid.argtypes = [i32]
     L.pq3d_ens_step.argtypes = [vp, i32, vp]
     for f in ("pq3d_src_records", "pq3d_hs_records", "pq3d_traction_pairs", "pq3d_stress_points", "pq3d_dense_assemble",
-              "pq3d_aca_batched", "pq3d_aca_pack", "pq3d_hmatvec", "pq3d_rk_grid", "pq3d_rk_step", "pq3d_ens_grid",
+              "pq3d_aca_batched", "pq3d_aca_pack", "pq3d_hmatvec", "pq3d_nearfield_rowabs", "pq3d_aca_term_weights",
+              "pq3d_aca_pack_mixed", "pq3d_rk_grid", "pq3d_rk_step", "pq3d_ens_grid",
               "pq3d_ens_step", "pq3d_ens_task_rows", "pq3d_rk_rows_attempt", "pq3d_rk_rows_accept",
               "pq3d_host_map_alloc", "pq3d_host_map_free", "pq3d_event_create", "pq3d_event_destroy",
               "pq3d_event_record", "pq3d_event_sync", "pq3d_event_query", "pq3d_snapshot", "pq3d_stream_wait_event"):
         getattr(L, f).restype = ctypes.c_int
     sizes = {"DenseItem": (L.pq3d_item_bytes(0), DENSE_ITEM.itemsize), "VItem": (L.pq3d_item_bytes(1), V_ITEM.itemsize),
-             "UTask": (L.pq3d_item_bytes(2), U_TASK.itemsize),
+             "UTask": (L.pq3d_item_bytes(2), U_TASK.itemsize), "UTaskM": (L.pq3d_item_bytes(6), U_TASK_M.itemsize),
+             "PackTaskM": (L.pq3d_pack_mixed_task_bytes(), PACK_TASK_M.itemsize),
              "DenseBlock": (L.pq3d_item_bytes(4), DENSE_BLOCK.itemsize), "HmPlan": (L.pq3d_item_bytes(5), HM_PLAN.itemsize),
              "AcaTask": (L.pq3d_aca_task_bytes(), ACA_TASK.itemsize), "PackTask": (L.pq3d_pack_task_bytes(), PACK_TASK.itemsize),
              "RkArgs": (L.pq3d_rk_args_bytes(), RK_ARGS.itemsize),

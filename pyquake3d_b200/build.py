@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpq3d.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
-SOURCES = ["gf.cu", "aca.cu", "hmatvec.cu", "rk.cu", "ensemble.cu", "vmode.cu", "mlp.cu", "hostio.cu"]
+SOURCES = ["gf.cu", "aca.cu", "hmatvec.cu", "mixed_pack.cu", "rk.cu", "ensemble.cu", "vmode.cu", "mlp.cu", "hostio.cu"]
 EXTRA = {}
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

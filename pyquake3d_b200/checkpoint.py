@@ -36,7 +36,8 @@ VERSION = 1
 ALIGN = 4096
 FILE_NAME = "operator.pq3d"
 
-_NP = {"float64": np.float64, "float32": np.float32, "int32": np.int32, "uint16": np.uint16, "uint8": np.uint8}
+_NP = {"float64": np.float64, "float32": np.float32, "int32": np.int32, "uint16": np.uint16, "uint8": np.uint8,
+       "int16": np.int16, "int8": np.int8}
 
 
 def fingerprint(xg, ev, mu, lam, mini_leaf, eta, min_size, aca_tol, aca_rel, aca_seed, kcap, layout, halfspace=0):
@@ -53,7 +54,7 @@ def fingerprint(xg, ev, mu, lam, mini_leaf, eta, min_size, aca_tol, aca_rel, aca
 def _layout(op):
     return dict(dense={str(k): v for k, v in op.DENSE_CHUNK_GROUPS.items()},
                 v={str(k): v for k, v in op.V_CHUNK_GROUPS.items()}, u_rows=op.U_ROWS,
-                dense_block=_lib.DENSE_BLOCK.itemsize)
+                dense_block=_lib.DENSE_BLOCK.itemsize, mixed_tol=float(getattr(op, "mixed_tol", 0.0)))
 
 
 def op_fingerprint(op, xg, ev):
@@ -85,6 +86,12 @@ def save_operator(op, path, xg, ev):
     for d in precisions:
         arrays.append(("U_" + d, _host(op.plans[d]["U"])))
         arrays.append(("V_" + d, _host(op.plans[d]["V"])))
+        if d == "mixed":
+            # the FP16 / INT8 class arrays, their scales and every term's class code
+            M = op.plans[d]["mixed"]
+            arrays += [("U16_mixed", _host(M["U"][1]).view(np.int16)), ("V16_mixed", _host(M["V"][1]).view(np.int16)),
+                       ("U8_mixed", _host(M["U"][2])), ("V8_mixed", _host(M["V"][2])),
+                       ("scales_mixed", _host(M["scales"])), ("tmap_mixed", np.asarray(op.mixed_tmap, np.int32))]
     table, off = [], 0
     for name, a in arrays:
         table.append(dict(name=name, dtype=str(a.dtype), count=int(a.size), offset=off))
@@ -146,6 +153,12 @@ def load_operator(op, path, xg, ev):
     op.task_ws = {}
     for d in header["precisions"]:
         U, V = _read(path, header, "U_" + d), _read(path, header, "V_" + d)
+        if d == "mixed":
+            t = lambda name, dt=None: torch.from_numpy(_read(path, header, name).copy()).to(op.dev)
+            op.install_mixed(_read(path, header, "tmap_mixed").copy(),
+                             [t("U_mixed"), t("U16_mixed").view(torch.float16), t("U8_mixed")],
+                             [t("V_mixed"), t("V16_mixed").view(torch.float16), t("V8_mixed")], t("scales_mixed"))
+            continue
         if d == "bf16":
             Ut = torch.from_numpy(U.view(np.int16)).to(op.dev).view(torch.bfloat16)
             Vt = torch.from_numpy(V.view(np.int16)).to(op.dev).view(torch.bfloat16)

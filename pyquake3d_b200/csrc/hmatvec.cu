@@ -28,6 +28,7 @@
 #include "pq3d_common.cuh"
 #include "hm_layout.cuh"
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <type_traits>
 
 using namespace pq3d;
@@ -45,6 +46,14 @@ struct Vec16<double> {
 template <>
 struct Vec16<__nv_bfloat16> {
     __nv_bfloat16 v[8];
+};
+template <>
+struct Vec16<__half> {
+    __half v[8];
+};
+template <>
+struct Vec16<int8_t> {
+    int8_t v[16];
 };
 
 template <typename T>
@@ -78,6 +87,10 @@ template <>
 __device__ __forceinline__ float tof<float>(float v) { return v; }
 template <>
 __device__ __forceinline__ float tof<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <>
+__device__ __forceinline__ float tof<__half>(__half v) { return __half2float(v); }
+template <>
+__device__ __forceinline__ float tof<int8_t>(int8_t v) { return (float)v; }
 
 template <typename TA, typename T>
 __device__ __forceinline__ TA widen(T v)
@@ -86,6 +99,46 @@ __device__ __forceinline__ TA widen(T v)
 }
 template <>
 __device__ __forceinline__ double widen<double, double>(double v) { return v; }
+
+// One V item: rows [q, q+nr) of a block's V (one slip), column groups [g0, g1):
+// chunk partials of t = V x.  lane = 8 * jg + rr: rows q + rr + 8u (u < 4),
+// column groups g0 + jg, g0 + jg + 4, ...; four rows per lane share each x slice.
+template <typename TL, typename TA>
+__device__ __forceinline__ void v_item(const VItem &it, int slip, const TL *__restrict__ Vd,
+                                       const TA *__restrict__ x, int xstride, TA *__restrict__ tpart)
+{
+    constexpr int CWV = 16 / sizeof(TL);
+    const int lane = threadIdx.x & 31;
+    const int rr = lane & 7, jg = lane >> 3;
+    TA acc[4] = {0, 0, 0, 0};
+    if (rr < it.nr) {
+        const TL *p = Vd + it.off + ((int64_t)(it.g0 + jg) * it.Q + it.q + rr) * CWV;
+        const int64_t gstride = (int64_t)4 * it.Q * CWV;
+        const TA *xp = x + (int64_t)(2 + slip) * xstride + it.c0 + (int64_t)(it.g0 + jg) * CWV;  // CWV-aligned
+        const int nu = (it.nr - rr + 7) >> 3;   // rows of this lane (1..4)
+#pragma unroll 2
+        for (int g = it.g0 + jg; g < it.g1; g += 4) {
+            TA xs[CWV];
+            ld_vec<TA, CWV>(xp, xs);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (u < nu) {
+                    Vec16<TL> d = ld_stream(p + 8 * u * CWV);
+#pragma unroll
+                    for (int t = 0; t < CWV; ++t) acc[u] += widen<TA>(d.v[t]) * xs[t];
+                }
+            }
+            p += gstride;
+            xp += 4 * CWV;
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], 8);
+        acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], 16);
+        if (jg == 0 && rr + 8 * u < it.nr) tpart[it.tp + it.q + rr + 8 * u] = acc[u];
+    }
+}
 
 // ------------------------------------------------------------------ kernel 1
 // Work item of warp w: dense items (lanes over block rows) first, then V items (up
@@ -99,7 +152,6 @@ __device__ __forceinline__ void dense_v_item(int64_t w, const DenseItem *__restr
                                              TA *__restrict__ tpart)
 {
     constexpr int CWD = 16 / sizeof(TD);
-    constexpr int CWV = 16 / sizeof(TL);
     const int lane = threadIdx.x & 31;
     if (w < n_ditems) {
         const DenseItem it = ditems[w];
@@ -136,38 +188,7 @@ __device__ __forceinline__ void dense_v_item(int64_t w, const DenseItem *__restr
     }
     const int64_t wv = w - n_ditems;
     if (wv >= n_vitems) return;
-    const VItem it = vitems[wv];
-    // lane = 8 * jg + rr: rows q + rr + 8u (u < 4), column groups g0 + jg, g0 + jg + 4, ...
-    // Four rows per lane share each x slice.
-    const int rr = lane & 7, jg = lane >> 3;
-    TA acc[4] = {0, 0, 0, 0};
-    if (rr < it.nr) {
-        const TL *p = Vd + it.off + ((int64_t)(it.g0 + jg) * it.Q + it.q + rr) * CWV;
-        const int64_t gstride = (int64_t)4 * it.Q * CWV;
-        const TA *xp = x + (int64_t)(2 + it.s) * xstride + it.c0 + (int64_t)(it.g0 + jg) * CWV;  // CWV-aligned
-        const int nu = (it.nr - rr + 7) >> 3;   // rows of this lane (1..4)
-#pragma unroll 2
-        for (int g = it.g0 + jg; g < it.g1; g += 4) {
-            TA xs[CWV];
-            ld_vec<TA, CWV>(xp, xs);
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (u < nu) {
-                    Vec16<TL> d = ld_stream(p + 8 * u * CWV);
-#pragma unroll
-                    for (int t = 0; t < CWV; ++t) acc[u] += widen<TA>(d.v[t]) * xs[t];
-                }
-            }
-            p += gstride;
-            xp += 4 * CWV;
-        }
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], 8);
-        acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], 16);
-        if (jg == 0 && rr + 8 * u < it.nr) tpart[it.tp + it.q + rr + 8 * u] = acc[u];
-    }
+    v_item<TL, TA>(vitems[wv], vitems[wv].s, Vd, x, xstride, tpart);
 }
 
 // Kernel A: V items (and, in FP64, the dense items), one warp each.  Every CTA
@@ -225,6 +246,15 @@ __device__ __forceinline__ void smem_vec<float, 4>(const float *p, float *o)
 {
     const float4 a = reinterpret_cast<const float4 *>(p)[0];
     o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+}
+template <>
+__device__ __forceinline__ void smem_vec<float, 16>(const float *p, float *o)
+{
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float4 a = reinterpret_cast<const float4 *>(p)[k];
+        o[4 * k] = a.x; o[4 * k + 1] = a.y; o[4 * k + 2] = a.z; o[4 * k + 3] = a.w;
+    }
 }
 template <>
 __device__ __forceinline__ void smem_vec<double, 2>(const double *p, double *o)
@@ -345,6 +375,116 @@ k_u(const UTask *__restrict__ tasks, const TL *__restrict__ U, const TA *__restr
     }
 }
 
+// ------------------------------------------------------------------ mixed storage
+// Storage code 3: FP32 dense near field; each low-rank block's ACA terms split
+// into three classes stored as FP32, FP16 and INT8 (class arrays U_c, V_c in
+// the layouts of hm_layout.cuh with CW = 4, 8, 16).  FP16 and INT8 columns of U
+// and rows of V are stored normalised to their largest magnitude (INT8 as
+// round(127 v / max)); the product's scale, one float per V row, multiplies the
+// row's sum of chunk partials when a U task gathers t.  FP32 terms are stored
+// as in the FP32 plan.  V items carry their class in bits 8+ of VItem::s.
+struct UTaskM {
+    int64_t off[3];            // block offsets in the FP32 / FP16 / INT8 U arrays
+    int32_t m, r0, r1, slot;   // rows [r0, r1) of an m-row block; slot of block row 0
+    int32_t K[3], kS[3], kD[3], Q[3], tp[3], nch[3], sb[3];  // per class (sb: scale base)
+    int32_t pad;
+};
+
+// acc[c] += sum_q U_c[r, q] t_c[q] over one class's column groups.
+template <typename TL>
+__device__ __forceinline__ void u_row_class(const TL *__restrict__ Ub, int m, int r, int K, const float *ts,
+                                            float acc[3])
+{
+    constexpr int CW = 16 / sizeof(TL);
+    const int ng = K / CW;
+    const TL *p = Ub + (int64_t)r * CW;                   // [group][comp][row][CW]
+    const int64_t cstride = (int64_t)m * CW, gstride = 3 * cstride;
+#pragma unroll 2
+    for (int g = 0; g < ng; ++g) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            Vec16<TL> d = ld_stream(p + c * cstride);
+            float tv[CW];
+            smem_vec<float, CW>(ts + c * K + g * CW, tv);
+#pragma unroll
+            for (int k = 0; k < CW; ++k) acc[c] += tof(d.v[k]) * tv[k];
+        }
+        p += gstride;
+    }
+}
+
+__device__ __forceinline__ void u_task_mixed(const UTaskM &T, const float *__restrict__ U32,
+                                             const __half *__restrict__ U16, const int8_t *__restrict__ U8,
+                                             const float *__restrict__ tpart, const float *__restrict__ scales,
+                                             float *__restrict__ slots, float *ts)
+{
+    const int base1 = 3 * T.K[0], base2 = 3 * (T.K[0] + T.K[1]);
+#pragma unroll
+    for (int cls = 0; cls < 3; ++cls) {
+        const int K = T.K[cls], kS = T.kS[cls], kD = T.kD[cls];
+        float *tc = ts + (cls == 0 ? 0 : (cls == 1 ? base1 : base2));
+        for (int e = threadIdx.x; e < 3 * K; e += blockDim.x) {
+            const int c = e / K, q = e % K;
+            int row = -1;
+            if (q < kS) row = c * kS + q;
+            else if (q < kS + kD) row = 3 * kS + c * kD + (q - kS);
+            float v = 0.f;
+            if (row >= 0) {
+                v = sum_partials<float>(tpart + T.tp[cls] + row, T.nch[cls], T.Q[cls]);
+                if (cls > 0) v *= scales[T.sb[cls] + row];
+            }
+            tc[e] = v;
+        }
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int rb = T.r0 + warp * 32; rb < T.r1; rb += blockDim.x) {
+        const int r = rb + lane;
+        if (r >= T.r1) break;
+        float acc[3] = {0.f, 0.f, 0.f};
+        if (T.K[0]) u_row_class<float>(U32 + T.off[0], T.m, r, T.K[0], ts, acc);
+        if (T.K[1]) u_row_class<__half>(U16 + T.off[1], T.m, r, T.K[1], ts + base1, acc);
+        if (T.K[2]) u_row_class<int8_t>(U8 + T.off[2], T.m, r, T.K[2], ts + base2, acc);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) slots[3 * ((int64_t)T.slot + r) + c] = acc[c];
+    }
+}
+
+// V items of all three classes, one warp each (the class picks the element type).
+__global__ void __launch_bounds__(256)
+k_v_mixed(const VItem *__restrict__ vitems, int64_t n_vitems, const float *__restrict__ V32,
+          const __half *__restrict__ V16, const int8_t *__restrict__ V8, const float *__restrict__ x, int xstride,
+          float *__restrict__ tpart)
+{
+    asm volatile("griddepcontrol.launch_dependents;");
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (w >= n_vitems) return;
+    const VItem it = vitems[w];
+    const int cls = it.s >> 8, slip = it.s & 255;
+    if (cls == 0) v_item<float, float>(it, slip, V32, x, xstride, tpart);
+    else if (cls == 1) v_item<__half, float>(it, slip, V16, x, xstride, tpart);
+    else v_item<int8_t, float>(it, slip, V8, x, xstride, tpart);
+}
+
+// Dense items, then the mixed U tasks (programmatic dependent launch after k_v_mixed,
+// as k_du after k_dense_v).
+__global__ void __launch_bounds__(256)
+k_du_mixed(const DenseItem *__restrict__ ditems, int64_t n_ditems, int64_t n_dblocks,
+           const UTaskM *__restrict__ tasks, const float *__restrict__ D, const float *__restrict__ U32,
+           const __half *__restrict__ U16, const int8_t *__restrict__ U8, const float *__restrict__ x,
+           float *__restrict__ slots, const float *__restrict__ tpart, const float *__restrict__ scales)
+{
+    if (blockIdx.x < n_dblocks) {
+        const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+        dense_v_item<float, float, float>(w, ditems, n_ditems, nullptr, 0, D, nullptr, x, 0, slots, nullptr);
+        return;
+    }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const UTaskM T = tasks[blockIdx.x - n_dblocks];
+    u_task_mixed(T, U32, U16, U8, tpart, scales, slots, reinterpret_cast<float *>(smraw));
+}
+
 // ------------------------------------------------------------------ kernel 3
 // y[3i+c] = sum of row i's slots (in list order) + add[c][i] (FP64), for rows of leaf clusters.
 template <typename TA>
@@ -394,7 +534,8 @@ __global__ void k_rowsum(int n, const int32_t *__restrict__ leaf_of_row, const i
 // Packed operator description (device pointers) -- mirrors the Python HM_PLAN record.
 struct HmPlan {
     int32_t n;             // elements
-    int32_t dtype;         // 0: FP64 dense + FP64 low rank; 1: FP32 + FP32; 2: FP32 dense + BF16 low rank
+    int32_t dtype;         // 0: FP64 dense + FP64 low rank; 1: FP32 + FP32; 2: FP32 dense + BF16 low rank;
+                           // 3: FP32 dense + FP32/FP16/INT8 low-rank term classes
     const void *dense;     // packed dense data
     const void *U;         // packed U factors
     const void *V;         // packed V factors
@@ -403,7 +544,10 @@ struct HmPlan {
     const void *utasks;    // UTask[n_utasks]
     const int32_t *leaf_of_row, *leaf_ptr, *leaf_off;
     int64_t n_ditems, n_vitems, n_utasks, n_slots, n_tpart;
-    int32_t kmax, pad;     // largest K of a low-rank block (shared memory of k_u)
+    int32_t kmax, pad;     // largest K of a low-rank block (shared memory of k_u); mixed: of K0+K1+K2
+    // storage code 3 only (U, V above are the FP32 class arrays)
+    const void *U16, *V16, *U8, *V8;   // FP16 and INT8 class arrays
+    const float *scales;               // per-V-row scales of the FP16 and INT8 classes
 };
 
 PQ3D_EXPORT size_t pq3d_item_bytes(int kind)
@@ -414,6 +558,7 @@ PQ3D_EXPORT size_t pq3d_item_bytes(int kind)
     case 2: return sizeof(UTask);
     case 4: return sizeof(DenseBlock);
     case 5: return sizeof(HmPlan);
+    case 6: return sizeof(UTaskM);
     }
     return 0;
 }
@@ -472,6 +617,45 @@ static int run_matvec(const HmPlan &P, const TA *x, TA *slots, TA *tpart, const 
     return pq3d_launch_status();
 }
 
+// Storage code 3: k_v_mixed (V items of every class), then k_du_mixed (dense items in
+// its tail, then the U tasks), then the optional row sum.
+static int run_matvec_mixed(const HmPlan &P, const float *x, float *slots, float *tpart, const double *add0,
+                            const double *add1, const double *add2, double *y, cudaStream_t st)
+{
+    if (P.n_vitems > 0) {
+        const int64_t blocks = (P.n_vitems * 32 + 255) / 256;
+        k_v_mixed<<<(unsigned)blocks, 256, 0, st>>>((const VItem *)P.vitems, P.n_vitems, (const float *)P.V,
+                                                    (const __half *)P.V16, (const int8_t *)P.V8, x, x_stride(P.n),
+                                                    tpart);
+    }
+    const int64_t n_dblocks = (P.n_ditems * 32 + 255) / 256;
+    const int64_t grid = n_dblocks + P.n_utasks;
+    if (grid > 0) {
+        const size_t smem = P.n_utasks > 0 ? (size_t)3 * P.kmax * sizeof(float) : 0;
+        if (smem > 200 * 1024) return PQ3D_ERR_ARG;
+        if (smem > 48 * 1024)
+            PQ3D_CHECK(cudaFuncSetAttribute(k_du_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)grid);
+        cfg.blockDim = dim3(256);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = P.n_vitems > 0 ? 1 : 0;
+        PQ3D_CHECK(cudaLaunchKernelEx(&cfg, k_du_mixed, (const DenseItem *)P.ditems, P.n_ditems, n_dblocks,
+                                      (const UTaskM *)P.utasks, (const float *)P.dense, (const float *)P.U,
+                                      (const __half *)P.U16, (const int8_t *)P.U8, x, slots, (const float *)tpart,
+                                      P.scales));
+    }
+    if (y)
+        k_rowsum<float><<<(P.n + 255) / 256, 256, 0, st>>>(P.n, P.leaf_of_row, P.leaf_ptr, P.leaf_off, slots, add0,
+                                                           add1, add2, y);
+    return pq3d_launch_status();
+}
+
 // y (n x 3, FP64, tree order) = K x (+ add_c).  x: deficit in the layout of hm_layout.cuh
 // (4 * x_stride(n) entries: interleaved, strike plane, dip plane), FP64 for dtype 0 and
 // FP32 otherwise.  Scratch: slots (3*n_slots) and
@@ -495,6 +679,10 @@ PQ3D_EXPORT int pq3d_hmatvec(const void *plan_host, const void *d_x, void *d_slo
     case 2:
         return run_matvec<float, __nv_bfloat16, float>(P, (const float *)d_x, (float *)d_slots, (float *)d_tpart,
                                                        d_add0, d_add1, d_add2, d_y, stream);
+    case 3:
+        if (P.n_utasks > 0 && (!P.U || !P.U16 || !P.U8 || !P.V || !P.V16 || !P.V8 || !P.scales)) return PQ3D_ERR_ARG;
+        return run_matvec_mixed(P, (const float *)d_x, (float *)d_slots, (float *)d_tpart, d_add0, d_add1, d_add2,
+                                d_y, stream);
     }
     return PQ3D_ERR_ARG;
 }

@@ -235,19 +235,8 @@ def build_plan_arrays(struct, dense_recs, kS, kD, code, dense_chunk=64, v_chunk=
     cluster, the offsets s - r0 of all slot owners covering that leaf."""
     cwd, cwl = _CW_DENSE[code], _CW_LR[code]
     n = struct.n
-    ditems, slot_rows = [], []
-    slot = 0
     dense_off = dense_recs["off64"] if code == 0 else dense_recs["off32"]
-    for i in range(len(dense_recs)):
-        m, nn, r0, c0 = (int(dense_recs[k][i]) for k in ("m", "n", "r0", "c0"))
-        lead = c0 % cwd
-        ng = _cdiv(nn + lead, cwd)
-        for g0 in range(0, ng, dense_chunk):
-            g1 = min(ng, g0 + dense_chunk)
-            for r in range(0, m, 32):
-                ditems.append((int(dense_off[i]), m, r, g0, g1, c0 - lead, slot))
-            slot_rows.append((slot, r0, m))
-            slot += m
+    ditems, slot_rows, slot = _dense_items(dense_recs, cwd, dense_off, dense_chunk)
     aca_blocks = [b for b in struct.blocks if b.aca]
     u_off = v_off = tp = 0
     vitems, utasks, pack = [], [], []
@@ -283,6 +272,38 @@ def build_plan_arrays(struct, dense_recs, kS, kD, code, dense_chunk=64, v_chunk=
         tp += nch * Q
         u_off += (K // cwl) * m * 3 * cwl
         v_off += Q * npad
+    L = _leaf_lists(struct, slot_rows)
+    esz_d = 8 if code == 0 else 4
+    esz_l = {0: 8, 1: 4, 2: 2}[code]
+    dense_entries = int(np.sum(dense_recs["m"].astype(np.int64) * dense_recs["n"])) if len(dense_recs) else 0
+    return dict(ditems=_rec(ditems, _lib.DENSE_ITEM), vitems=_rec(vitems, _lib.V_ITEM),
+                utasks=_rec(utasks, _lib.U_TASK),
+                n_ditems=len(ditems), n_vitems=len(vitems), n_utasks=len(utasks), n_slots=slot, n_tpart=tp, kmax=kmax,
+                u_size=u_off, v_size=v_off, pack=pack, alg_bytes=dense_entries * 6 * esz_d + lr_entries * esz_l +
+                2 * n * esz_d + 3 * n * 8, **L)
+
+
+def _dense_items(dense_recs, cwd, dense_off, dense_chunk):
+    """Dense work items (one warp: 32 rows x a chunk of column groups) and their slots:
+    every (block, column chunk) owns m consecutive slots."""
+    ditems, slot_rows = [], []
+    slot = 0
+    for i in range(len(dense_recs)):
+        m, nn, r0, c0 = (int(dense_recs[k][i]) for k in ("m", "n", "r0", "c0"))
+        lead = c0 % cwd
+        ng = _cdiv(nn + lead, cwd)
+        for g0 in range(0, ng, dense_chunk):
+            g1 = min(ng, g0 + dense_chunk)
+            for r in range(0, m, 32):
+                ditems.append((int(dense_off[i]), m, r, g0, g1, c0 - lead, slot))
+            slot_rows.append((slot, r0, m))
+            slot += m
+    return ditems, slot_rows, slot
+
+
+def _leaf_lists(struct, slot_rows):
+    """Per leaf cluster, the offsets (slot - first row) of every slot owner covering it."""
+    n = struct.n
     nleaf = len(struct.leaves)
     leaf_of_row = np.empty(n, dtype=np.int32)
     for lf in struct.leaves:
@@ -298,24 +319,127 @@ def build_plan_arrays(struct, dense_recs, kS, kD, code, dense_chunk=64, v_chunk=
     leaf_ptr = np.zeros(nleaf + 1, dtype=np.int64)
     np.add.at(leaf_ptr, rep_leaf + 1, 1)
     leaf_ptr = np.cumsum(leaf_ptr).astype(np.int32)
+    return dict(leaf_of_row=leaf_of_row, leaf_ptr=leaf_ptr,
+                leaf_off=leaf_off if len(leaf_off) else np.zeros(1, np.int32), slot_rows=sr)
 
-    def rec(rows, dt):
-        return np.array(rows, dtype=dt) if rows else np.zeros(1, dtype=dt)
 
-    esz_d = 8 if code == 0 else 4
-    esz_l = {0: 8, 1: 4, 2: 2}[code]
+# ----------------------------------------------------------------------------- mixed storage (host)
+
+MIXED_CW = (4, 8, 16)               # column groups of the FP32 / FP16 / INT8 term classes
+MIXED_BYTES = (4, 2, 1)
+# relative rounding of a stored entry against its vector's largest magnitude
+MIXED_EPS = (2.0 ** -24, 2.0 ** -11, 0.5 / 127.0)
+
+
+def classify_terms(wS, wD, tol):
+    """Classes (0 FP32, 1 FP16, 2 INT8) of one block's ACA terms from their weights
+    w = max_i(|u_i| / R_i) ||v||_1 (strike terms wS, dip terms wD, in ACA order).
+
+    A term needs FP32 when 2 eps_FP16 w > tol (quantising u and v to FP16 would move a
+    row by more than tol times its near-field absolute row sum), FP16 when 2 eps_INT8 w
+    > tol, else INT8 suffices.  Each class's column count is padded to its column
+    group (4, 8, 16); the padding is filled by promoting the next most important terms
+    instead of storing zeros, and an INT8 remnant of at most 8 terms (or an FP16
+    remnant of at most 4 after FP32 and with no INT8 terms) moves up a class at no
+    extra storage.  Returns (cls_S, cls_D) arrays of class codes."""
+    w = np.concatenate([np.asarray(wS, dtype=np.float64), np.asarray(wD, dtype=np.float64)])
+    K = len(w)
+    if K == 0:
+        return np.zeros(0, np.int32), np.zeros(0, np.int32)
+    req = np.where(2 * MIXED_EPS[1] * w > tol, 0, np.where(2 * MIXED_EPS[2] * w > tol, 1, 2))
+    n0, n1 = int((req == 0).sum()), int((req == 1).sum())
+    n0p = min(K, _cdiv(n0, 4) * 4) if n0 else 0
+    rem1 = max(0, n0 + n1 - n0p)
+    left = K - n0p
+    n1p = min(left, _cdiv(rem1, 8) * 8) if rem1 else 0
+    n2p = left - n1p
+    if 0 < n2p <= 8:
+        n1p, n2p = n1p + n2p, 0
+    if n2p == 0 and 0 < n1p <= 4 and n0p % 4 == 0:
+        n0p, n1p = n0p + n1p, 0
+    order = np.argsort(-w, kind="stable")
+    cls = np.empty(K, np.int32)
+    cls[order[:n0p]] = 0
+    cls[order[n0p:n0p + n1p]] = 1
+    cls[order[n0p + n1p:]] = 2
+    return cls[:len(wS)], cls[len(wS):]
+
+
+def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chunk=32, u_rows=512):
+    """Work items, slot layout and packing records of the mixed storage (code 3):
+    FP32 dense items as in the FP32 plan; per low-rank block and term class c
+    (FP32, FP16, INT8) the class's own U / V arrays with column groups MIXED_CW[c].
+    cls_lists[bi] = (cls_S, cls_D) from classify_terms.  Pure numpy."""
+    ditems, slot_rows, slot = _dense_items(dense_recs, 4, dense_recs["off32"], dense_chunk)
+    aca_blocks = [b for b in struct.blocks if b.aca]
+    u_off, v_off = [0, 0, 0], [0, 0, 0]
+    tp = sb = 0
+    vitems, utasks, pack = [], [], []
+    lr_bytes = 0
+    kmax = 0
+    counts = np.zeros((3, 2), np.int64)      # terms per (class, slip)
+    for bi, b in enumerate(aca_blocks):
+        m, nn = len(b.row.indices), len(b.col.indices)
+        lo, hi = getattr(b, "rows", (0, m))
+        cS, cD = cls_lists[bi]
+        ks = [int((cS == c).sum()) for c in range(3)]
+        kd = [int((cD == c).sum()) for c in range(3)]
+        if sum(ks) + sum(kd) == 0:
+            continue
+        Ks = [_cdiv(ks[c] + kd[c], MIXED_CW[c]) * MIXED_CW[c] for c in range(3)]
+        Qs = [3 * (ks[c] + kd[c]) for c in range(3)]
+        kmax = max(kmax, sum(Ks))
+        rec_off, rec_tp, rec_nch, rec_sb, rec_voff = [0] * 3, [0] * 3, [0] * 3, [0] * 3, [0] * 3
+        for c in range(3):
+            counts[c] += (ks[c], kd[c])
+            cw = MIXED_CW[c]
+            lr_bytes += Qs[c] * ((hi - lo) + nn) * MIXED_BYTES[c] + (Qs[c] * 4 if c else 0)
+            rec_off[c], rec_voff[c] = u_off[c], v_off[c]
+            if Ks[c] == 0:
+                continue
+            lead = b.col.start % cw
+            ngv = _cdiv(nn + lead, cw)
+            nch = _cdiv(ngv, v_chunk)
+            for ch in range(nch):
+                g0, g1 = ch * v_chunk, min(ngv, (ch + 1) * v_chunk)
+                for s_, (qa, qb) in enumerate(((0, 3 * ks[c]), (3 * ks[c], Qs[c]))):
+                    for q in range(qa, qb, 32):
+                        vitems.append((v_off[c], Qs[c], q, min(32, qb - q), g0, g1, b.col.start - lead,
+                                       s_ | (c << 8), tp + ch * Qs[c]))
+            rec_tp[c], rec_nch[c] = tp, nch
+            tp += nch * Qs[c]
+            if c:
+                rec_sb[c] = sb
+                sb += Qs[c]
+            u_off[c] += Ks[c] * m * 3
+            v_off[c] += Qs[c] * ngv * cw
+        for r0 in range(lo, hi, u_rows):
+            utasks.append((rec_off, m, r0, min(hi, r0 + u_rows), slot - lo, Ks, ks, kd, Qs, rec_tp, rec_nch, rec_sb, 0))
+        slot_rows.append((slot, b.row.start + lo, hi - lo))
+        for p in (0, 1):
+            pack.append((bi, p, rec_off, rec_voff, ks, kd, Qs, Ks, rec_sb))
+        slot += hi - lo
+    A = _leaf_lists(struct, slot_rows)
     dense_entries = int(np.sum(dense_recs["m"].astype(np.int64) * dense_recs["n"])) if len(dense_recs) else 0
-    return dict(ditems=rec(ditems, _lib.DENSE_ITEM), vitems=rec(vitems, _lib.V_ITEM), utasks=rec(utasks, _lib.U_TASK),
-                n_ditems=len(ditems), n_vitems=len(vitems), n_utasks=len(utasks), n_slots=slot, n_tpart=tp, kmax=kmax,
-                u_size=u_off, v_size=v_off, pack=pack, leaf_of_row=leaf_of_row, leaf_ptr=leaf_ptr,
-                leaf_off=leaf_off if len(leaf_off) else np.zeros(1, np.int32), slot_rows=sr,
-                alg_bytes=dense_entries * 6 * esz_d + lr_entries * esz_l + 2 * n * esz_d + 3 * n * 8)
+    n = struct.n
+    A.update(ditems=_rec(ditems, _lib.DENSE_ITEM), vitems=_rec(vitems, _lib.V_ITEM),
+             utasks=_rec(utasks, _lib.U_TASK_M), n_ditems=len(ditems), n_vitems=len(vitems), n_utasks=len(utasks),
+             n_slots=slot, n_tpart=tp, n_scales=sb, kmax=kmax, u_sizes=u_off, v_sizes=v_off, pack=pack,
+             class_terms=counts, alg_bytes=dense_entries * 6 * 4 + lr_bytes + 2 * n * 4 + 3 * n * 8)
+    return A
+
+
+def _rec(rows, dt):
+    return np.array(rows, dtype=dt) if rows else np.zeros(1, dtype=dt)
 
 
 # ----------------------------------------------------------------------------- device operator
 
-DTYPES = {"fp64": 0, "fp32": 1, "bf16": 2}
-_CW_DENSE = {0: 2, 1: 4, 2: 4}
+DTYPES = {"fp64": 0, "fp32": 1, "bf16": 2, "mixed": 3}
+# default term-class tolerance of the mixed storage: a quantised term may move a row
+# by at most 2^-22 of its near-field absolute row sum (4 ulps of FP32 storage)
+MIXED_TOL = 2.0 ** -22
+_CW_DENSE = {0: 2, 1: 4, 2: 4, 3: 4}
 _CW_LR = {0: 2, 1: 4, 2: 8}
 
 
@@ -337,10 +461,13 @@ class DeviceHMatrix:
     U_ROWS = 512                                 # rows per U task (one CTA)
 
     def __init__(self, struct, xg, ev, nodes, tri, mu, lam, device="cuda", aca_tol=0.01, aca_rel=False,
-                 aca_seed=0, kcap=96, ws_budget_bytes=8 << 30, keep_factors=False, halfspace=0):
+                 aca_seed=0, kcap=96, ws_budget_bytes=8 << 30, keep_factors=False, halfspace=0,
+                 mixed_tol=MIXED_TOL):
         """halfspace: 0 full space; 1 half space, a triangle side along z adds no
         free-surface term; 2 half space with the side handling of the reference's
-        compiled library (the values its H-matrix assembly uses)."""
+        compiled library (the values its H-matrix assembly uses).  mixed_tol: the
+        term-class tolerance of the "mixed" storage (classify_terms)."""
+        self.mixed_tol = float(mixed_tol)
         import torch
         self.torch = torch
         self.L = _lib.load()
@@ -406,7 +533,7 @@ class DeviceHMatrix:
     def _assemble_dense(self, want):
         torch = self.torch
         need64 = "fp64" in want
-        need32 = any(d in want for d in ("fp32", "bf16"))
+        need32 = any(d in want for d in ("fp32", "bf16", "mixed"))
         recs, off64, off32 = dense_layout(self.dense_blocks)
         order = np.argsort(-(recs["m"].astype(np.int64) * recs["n"]), kind="stable")
         self.dense_recs = recs
@@ -520,6 +647,8 @@ class DeviceHMatrix:
                                  "assemble(want=...) or construct with keep_factors=True")
         torch = self.torch
         code = DTYPES[dtype]
+        if code == 3:
+            return self._plan_mixed()
         A = self.plan_arrays(dtype)
         lr_dtype = torch.float64 if code == 0 else (torch.float32 if code == 1 else torch.bfloat16)
         Ubuf = torch.zeros(max(A["u_size"], 8), dtype=lr_dtype, device=self.dev)
@@ -550,6 +679,111 @@ class DeviceHMatrix:
         pick = lambda v: v[code] if isinstance(v, dict) else v
         return build_plan_arrays(self.s, self.dense_recs, kS, kD, code, pick(self.DENSE_CHUNK_GROUPS),
                                  pick(self.V_CHUNK_GROUPS), self.U_ROWS)
+
+    def _task_records_mixed(self, keep_ws):
+        """PackTaskM records (per workspace batch) for every ACA task, with the weight /
+        term-map offset of each task (tasks in block order, strike pass first)."""
+        ro_np = self._row_offsets()
+        recs, tmap_off = {}, 0
+        offs = np.zeros(len(self.aca_tasks) + 1, np.int64)
+        for ti in range(len(self.aca_tasks)):
+            bi, p = divmod(ti, 2)
+            k = int(self.aca_ranks[ti])
+            offs[ti] = tmap_off
+            wi, wo, kmax = self.task_ws[ti]
+            b = self.aca_blocks[bi]
+            r = np.zeros(1, dtype=_lib.PACK_TASK_M)
+            r["ws_off"], r["rows_off"], r["cols_off"], r["tmap_off"] = wo, ro_np[bi][0], ro_np[bi][1], tmap_off
+            r["m"], r["n"], r["kmax"], r["k"], r["pass_"] = len(b.row.indices), len(b.col.indices), kmax, k, p
+            r["r0"], r["c0"], r["zeroB"] = b.row.start, b.col.start, 1 if self.aca_flags[ti] & 2 else 0
+            recs.setdefault(wi, []).append((ti, r))
+            tmap_off += k
+        offs[-1] = tmap_off
+        return recs, offs
+
+    def _plan_mixed(self):
+        """Mixed storage (code 3): FP32 dense near field; ACA terms in FP32 / FP16 / INT8
+        classes chosen from their weights against the near-field row sums."""
+        torch = self.torch
+        if self.dense32 is None:
+            raise _lib.Pq3dError("the mixed plan needs the FP32 dense blocks: request it in assemble(want=...)")
+        n = self.n
+        L = self.L
+        st = self._stream
+        # near-field absolute row sums (tree order), largest component
+        R3 = torch.zeros(3 * n, dtype=torch.float64, device=self.dev)
+        recs = self.dense_recs
+        if len(recs):
+            d_recs = torch.from_numpy(np.ascontiguousarray(recs).view(np.uint8)).to(self.dev)
+            check(L.pq3d_nearfield_rowabs(ptr(self.dense32), ptr(d_recs), len(recs), n, ptr(R3), st),
+                  "pq3d_nearfield_rowabs")
+        R = R3.view(3, n).max(dim=0).values.contiguous()
+        by_ws, offs = self._task_records_mixed(None)
+        w = torch.zeros(max(int(offs[-1]), 1), dtype=torch.float64, device=self.dev)
+        for wi, rows in by_ws.items():
+            rec = np.concatenate([r for _, r in rows])
+            d_rec = torch.from_numpy(rec.view(np.uint8)).to(self.dev)
+            check(L.pq3d_aca_term_weights(ptr(d_rec), len(rec), ptr(self.aca_ws[wi][0]), ptr(self.rowlist),
+                                          ptr(self.iperm), ptr(R), ptr(w), st), "pq3d_aca_term_weights")
+        w = w.cpu().numpy()
+        # classes per block, then each term's position within its class (per pass)
+        tmap = np.zeros(max(int(offs[-1]), 1), np.int32)
+        cls_lists = []
+        for bi in range(len(self.aca_blocks)):
+            tS, tD = 2 * bi, 2 * bi + 1
+            cS, cD = classify_terms(w[offs[tS]:offs[tS + 1]], w[offs[tD]:offs[tD + 1]], self.mixed_tol)
+            cls_lists.append((cS, cD))
+            for ti, cc in ((tS, cS), (tD, cD)):
+                pos = np.zeros(len(cc), np.int32)
+                for c in range(3):
+                    sel = np.nonzero(cc == c)[0]
+                    pos[sel] = np.arange(len(sel))
+                tmap[offs[ti]:offs[ti + 1]] = cc | (pos << 2)
+        self.mixed_tmap = tmap[:int(offs[-1])]
+        A = self._mixed_arrays(cls_lists)
+        tdt = (torch.float32, torch.float16, torch.int8)
+        Ub = [torch.zeros(max(int(A["u_sizes"][c]), 16), dtype=tdt[c], device=self.dev) for c in range(3)]
+        Vb = [torch.zeros(max(int(A["v_sizes"][c]), 16), dtype=tdt[c], device=self.dev) for c in range(3)]
+        scales = torch.zeros(max(A["n_scales"], 4), dtype=torch.float32, device=self.dev)
+        d_tmap = torch.from_numpy(tmap).to(self.dev)
+        layout = {}
+        for (bi, p, uo, vo, ks, kd, Q, K, sb) in A["pack"]:
+            layout[2 * bi + p] = (uo, vo, ks, kd, Q, K, sb)
+        for wi, rows in by_ws.items():
+            recl = []
+            for ti, r in rows:
+                if ti not in layout:
+                    continue                       # a block without terms
+                uo, vo, ks, kd, Q, K, sb = layout[ti]
+                r = r.copy()
+                r["u_off"], r["v_off"], r["kS"], r["kD"], r["Q"], r["K"], r["sb"] = uo, vo, ks, kd, Q, K, sb
+                recl.append(r)
+            if not recl:
+                continue
+            rec = np.concatenate(recl)
+            d_rec = torch.from_numpy(rec.view(np.uint8)).to(self.dev)
+            check(L.pq3d_aca_pack_mixed(ptr(d_rec), len(rec), ptr(self.aca_ws[wi][0]), ptr(self.rowlist),
+                                        ptr(self.collist), ptr(self.iperm), ptr(d_tmap), ptr(Ub[0]), ptr(Ub[1]),
+                                        ptr(Ub[2]), ptr(Vb[0]), ptr(Vb[1]), ptr(Vb[2]), ptr(scales), st),
+                  "pq3d_aca_pack_mixed")
+        A["mixed"] = dict(U=Ub, V=Vb, scales=scales, tol=self.mixed_tol, class_terms=A["class_terms"].tolist())
+        return self._finish_plan("mixed", A, Ub[0], Vb[0])
+
+    def _mixed_arrays(self, cls_lists):
+        return build_plan_arrays_mixed(self.s, self.dense_recs, cls_lists, self.DENSE_CHUNK_GROUPS[1],
+                                       self.V_CHUNK_GROUPS[1], self.U_ROWS)
+
+    def install_mixed(self, tmap, U, V, scales):
+        """Register a mixed plan whose class arrays come from elsewhere (an operator
+        checkpoint): tmap holds every term's class code (bits 0-1) in task order."""
+        offs = np.concatenate([[0], np.cumsum(np.asarray(self.aca_ranks, np.int64))])
+        cls_lists = [(tmap[offs[2 * bi]:offs[2 * bi + 1]] & 3, tmap[offs[2 * bi + 1]:offs[2 * bi + 2]] & 3)
+                     for bi in range(len(self.aca_blocks))]
+        self.mixed_tmap = np.asarray(tmap, np.int32)
+        A = self._mixed_arrays(cls_lists)
+        A["mixed"] = dict(U=list(U), V=list(V), scales=scales, tol=self.mixed_tol,
+                          class_terms=A["class_terms"].tolist())
+        return self._finish_plan("mixed", A, U[0], V[0])
 
     def install_plan(self, dtype, Ubuf, Vbuf):
         """Register a plan whose packed low-rank buffers were produced elsewhere (an
@@ -584,10 +818,18 @@ class DeviceHMatrix:
             hp[k] = P[k].data_ptr() if P[k] is not None else 0
         for k in ("n_ditems", "n_vitems", "n_utasks", "n_slots", "n_tpart", "kmax"):
             hp[k] = P[k]
+        if code == 3:
+            M = A["mixed"]
+            P["mixed"] = M
+            hp["U16"], hp["U8"] = M["U"][1].data_ptr(), M["U"][2].data_ptr()
+            hp["V16"], hp["V8"] = M["V"][1].data_ptr(), M["V"][2].data_ptr()
+            hp["scales"] = M["scales"].data_ptr()
         P["host_plan"] = hp
         P["alg_bytes"] = A["alg_bytes"]
         P["stored_bytes"] = (P["dense"].numel() * P["dense"].element_size() if P["dense"] is not None else 0) + \
             Ubuf.numel() * Ubuf.element_size() + Vbuf.numel() * Vbuf.element_size()
+        if code == 3:
+            P["stored_bytes"] += sum(t.numel() * t.element_size() for t in P["mixed"]["U"][1:] + P["mixed"]["V"][1:])
         self.plans[dtype] = P
         return P
 

@@ -31,7 +31,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import ptr, check
-from .hmatrix import HStructure, DeviceHMatrix
+from .hmatrix import HStructure, DeviceHMatrix, MIXED_TOL
 from .mesh import get_eleVec, find_boundary_edges_and_nodes
 
 
@@ -427,8 +427,10 @@ class BlockTree:
         tol = float(P.get("ACA tolerance", 0.01))
         rel = P.get("ACA relative tolerance", "False") == "True"
         seed = int(P.get("ACA seed", 0))
+        mtol = float(P.get("Mixed precision tolerance", MIXED_TOL))
         return DeviceHMatrix(self.struct, sim.xg, sim.eleVec, sim.nodelst, sim.elelst, sim.mu, sim.lambda_,
-                             device=sim.device, aca_tol=tol, aca_rel=rel, aca_seed=seed, halfspace=hs_mode(sim))
+                             device=sim.device, aca_tol=tol, aca_rel=rel, aca_seed=seed, halfspace=hs_mode(sim),
+                             mixed_tol=mtol)
 
     def master(self, dir=None, blocks_to_process=None, num_workers=None, save_corefunc=False):
         """Assemble every block on the GPU (dense near field + batched ACA); with

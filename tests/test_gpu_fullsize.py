@@ -51,7 +51,7 @@ def _case(name, tmp_path_factory, precision):
 @pytest.fixture(scope="module")
 def c60(lib, tmp_path_factory):
     sim = _case("curved60k", tmp_path_factory, "fp32")
-    sim.tree_block.want = ("fp64", "fp32", "bf16")
+    sim.tree_block.want = ("fp64", "fp32", "bf16", "mixed")
     return sim, sim.tree_block.op()
 
 
@@ -89,7 +89,7 @@ def test_sampled_rows_match_exact_operator(lib, c60):
     G = _exact_rows(lib, sim, rows)
     X1, X2 = torch.tensor(x1, device="cuda"), torch.tensor(x2, device="cuda")
     exact = [(G[c] @ X1 + G[c + 3] @ X2).cpu().numpy() for c in range(3)]
-    for dtype, tol in (("fp64", 20 * eps), ("fp32", 20 * eps)):
+    for dtype, tol in (("fp64", 20 * eps), ("fp32", 20 * eps), ("mixed", 20 * eps)):
         y = op.apply(x1, x2, dtype)
         for c in range(3):
             err = np.linalg.norm(y[c][rows] - exact[c]) / np.linalg.norm(exact[c])
@@ -101,7 +101,7 @@ def test_matvec_linearity_and_determinism(c60):
     n = op.n
     rng = np.random.default_rng(12)
     a, b = rng.standard_normal((2, 2, n)) * 1e-9
-    for dtype, tol in (("fp64", 1e-12), ("fp32", 1e-5), ("bf16", 1e-5)):
+    for dtype, tol in (("fp64", 1e-12), ("fp32", 1e-5), ("bf16", 1e-5), ("mixed", 1e-5)):
         ya = np.array(op.apply(a[0], a[1], dtype))
         yb = np.array(op.apply(b[0], b[1], dtype))
         yab = np.array(op.apply(a[0] + 2 * b[0], a[1] + 2 * b[1], dtype))
@@ -130,14 +130,15 @@ def test_graph_equals_eager_steps(c60):
         assert np.array_equal(sa[k], sb[k]), k
 
 
-def test_fp32_operator_within_slip_target_of_fp64(c60):
+@pytest.mark.parametrize("prec", ["fp32", "mixed"])
+def test_operator_within_slip_target_of_fp64(c60, prec):
     """On the FP64 run's step sizes (dt replay), 100 steps: slip relative L2
-    error of the FP32-operator run below the 1e-5 target."""
+    error of the FP32- and mixed-storage runs below the 1e-5 target."""
     from pyquake3d_b200.qdsim import DeviceStepper
     sim, op = c60
     ref = DeviceStepper(sim, op, "fp64")
     h = ref.run(100, sim.htry)[:, 0]
-    mix = DeviceStepper(sim, op, "fp32")
+    mix = DeviceStepper(sim, op, prec)
     mix.set_replay(torch.tensor(h, device="cuda"))
     mix.run(100, sim.htry)
     s64, s32 = ref.t["slip"].cpu().numpy(), mix.t["slip"].cpu().numpy()
@@ -265,24 +266,25 @@ def _pin_to_oracle(sim, op, nsteps=12):
                       ("slipv", "slipv")):
         r = getattr(ost, name)
         out["fp64_" + name] = float(np.abs(d64.get(dev) - r).max() / np.abs(r).max())
-    # FP32 operator on the oracle's step sizes
-    d32 = DeviceStepper(sim, op, "fp32")
-    d32.set_replay(torch.tensor(hs, dtype=torch.float64, device="cuda"))
-    d32.run(nsteps, sim.htry)
+    # FP32 and mixed operators on the oracle's step sizes
     rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
     slip_o = np.sqrt(ost.slip1 ** 2 + ost.slip2 ** 2)
-    out["fp32_slip"] = rel(np.sqrt(d32.get("slip1") ** 2 + d32.get("slip2") ** 2), slip_o)
-    out["fp32_V"] = rel(d32.get("slipv"), ost.slipv)
     th_o = _theta(ost.state, ost.dc, ost.f0, ost.b, sim.V0)
-    out["fp32_theta"] = rel(_theta(d32.get("psi"), ost.dc, ost.f0, ost.b, sim.V0), th_o)
+    for prec in [p for p in ("fp32", "mixed") if p in op.plans]:
+        d32 = DeviceStepper(sim, op, prec)
+        d32.set_replay(torch.tensor(hs, dtype=torch.float64, device="cuda"))
+        d32.run(nsteps, sim.htry)
+        out[prec + "_slip"] = rel(np.sqrt(d32.get("slip1") ** 2 + d32.get("slip2") ** 2), slip_o)
+        out[prec + "_V"] = rel(d32.get("slipv"), ost.slipv)
+        out[prec + "_theta"] = rel(_theta(d32.get("psi"), ost.dc, ost.f0, ost.b, sim.V0), th_o)
     return out
 
 
 def test_curved60k_pinned_to_oracle(c60):
     """curved60k: 12 adaptive steps of the oracle's simu_forward on the device's FP64
     operator (copied to the host) beside the device FP64 stepper (h to 1e-9, state
-    to 1e-8) and the FP32-operator stepper on the oracle's step sizes (slip, V and
-    theta relative L2 within the 1e-5 target)."""
+    to 1e-8) and the FP32- and mixed-storage steppers on the oracle's step sizes
+    (slip, V and theta relative L2 within the 1e-5 target)."""
     sim, op = c60
     e = _pin_to_oracle(sim, op)
     for k, v in e.items():
@@ -293,7 +295,7 @@ def test_curved60k_pinned_to_oracle(c60):
 def test_thrust20k_pinned_to_oracle(lib, tmp_path_factory):
     """thrust20k (20,480 triangles, ACA relative 1e-4): the same pin as curved60k."""
     sim = _case("thrust20k", tmp_path_factory, "fp32")
-    sim.tree_block.want = ("fp64", "fp32")
+    sim.tree_block.want = ("fp64", "fp32", "mixed")
     op = sim.tree_block.op()
     e = _pin_to_oracle(sim, op)
     for k, v in e.items():
