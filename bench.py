@@ -351,19 +351,29 @@ def ensemble_study(nsteps, nrep, faults=32):
                                  "alg_bytes": int(P["alg_bytes"])}}
         del g
     out["fp32_vs_fp64"] = out["fp32"]["fault_steps_per_s"] / out["fp64"]["fault_steps_per_s"]
-    # per-fault error: fresh ensembles from the initial state, FP32 on the FP64 step sizes
+    # per-fault error: fresh ensembles from the initial state, FP32 on the FP64 step sizes;
+    # beside it each fault's FP64 chaos floor (an FP64 run whose initial shear tractions
+    # differ by a relative 1e-12, on the same step sizes)
     R64 = Ensemble(sims, precision="fp64", share=E64)
     R32 = Ensemble(sims, precision="fp32", share=E64)
+    RP = Ensemble(sims, precision="fp64", share=E64)
+    RP.t["Tt1o"].mul_(1.0 + 1e-12)
     h = R64.run(nrep, h0)
-    R32.set_replay(torch.tensor(h[:, :, 0], device=R32.op.dev))
-    R32.run(nrep, h0)
-    errs = []
+    for R in (R32, RP):
+        R.set_replay(torch.tensor(h[:, :, 0], device=R.op.dev))
+        R.run(nrep, h0)
+    errs, floor = [], []
     for f in range(faults):
-        a, b = R32.get("slip", f), R64.get("slip", f)
-        errs.append(float(np.linalg.norm(a - b) / np.linalg.norm(b)))
+        b = R64.get("slip", f)
+        errs.append(float(np.linalg.norm(R32.get("slip", f) - b) / np.linalg.norm(b)))
+        floor.append(float(np.linalg.norm(RP.get("slip", f) - b) / np.linalg.norm(b)))
+    above = [f for f in range(faults) if errs[f] > 1e-5]
     out["slip_rel_err_vs_fp64"] = {"steps": nrep, "max": max(errs), "median": float(np.median(errs)),
-                                   "per_fault": errs, "method": "dt replay of the FP64 ensemble"}
-    del E32, E64, R32, R64
+                                   "per_fault": errs, "chaos_floor_per_fault": floor,
+                                   "above_1e-5": {str(f): {"fp32": errs[f], "chaos_floor": floor[f]} for f in above},
+                                   "method": "dt replay of the FP64 ensemble; chaos floor: FP64 with initial shear "
+                                             "tractions perturbed by a relative 1e-12"}
+    del E32, E64, R32, R64, RP
     torch.cuda.empty_cache()
     return out
 

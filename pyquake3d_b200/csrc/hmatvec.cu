@@ -52,8 +52,8 @@ struct Vec16<__half> {
     __half v[8];
 };
 template <>
-struct Vec16<int8_t> {
-    int8_t v[16];
+struct Vec16<uint8_t> {    // INT8 class: each byte holds b + 128, b in [-127, 127]
+    uint32_t w[4];
 };
 
 template <typename T>
@@ -89,8 +89,15 @@ template <>
 __device__ __forceinline__ float tof<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
 template <>
 __device__ __forceinline__ float tof<__half>(__half v) { return __half2float(v); }
-template <>
-__device__ __forceinline__ float tof<int8_t>(int8_t v) { return (float)v; }
+
+// Byte k (0..3) of w as the float 2^23 + byte, minus 2^23 + 128: the signed value
+// b of an INT8-class entry stored as b + 128, exactly, in one byte permute and one
+// add (the integer-to-float conversion instruction issues at a fraction of that rate).
+template <int k>
+__device__ __forceinline__ float i8_at(uint32_t w)
+{
+    return __int_as_float((int)__byte_perm(w, 0x4B000000u, 0x7650u + k)) - 8388736.0f;
+}
 
 template <typename TA, typename T>
 __device__ __forceinline__ TA widen(T v)
@@ -124,8 +131,18 @@ __device__ __forceinline__ void v_item(const VItem &it, int slip, const TL *__re
             for (int u = 0; u < 4; ++u) {
                 if (u < nu) {
                     Vec16<TL> d = ld_stream(p + 8 * u * CWV);
+                    if constexpr (std::is_same<TL, uint8_t>::value) {
 #pragma unroll
-                    for (int t = 0; t < CWV; ++t) acc[u] += widen<TA>(d.v[t]) * xs[t];
+                        for (int t = 0; t < 4; ++t) {
+                            acc[u] += i8_at<0>(d.w[t]) * xs[4 * t];
+                            acc[u] += i8_at<1>(d.w[t]) * xs[4 * t + 1];
+                            acc[u] += i8_at<2>(d.w[t]) * xs[4 * t + 2];
+                            acc[u] += i8_at<3>(d.w[t]) * xs[4 * t + 3];
+                        }
+                    } else {
+#pragma unroll
+                        for (int t = 0; t < CWV; ++t) acc[u] += widen<TA>(d.v[t]) * xs[t];
+                    }
                 }
             }
             p += gstride;
@@ -406,15 +423,25 @@ __device__ __forceinline__ void u_row_class(const TL *__restrict__ Ub, int m, in
             Vec16<TL> d = ld_stream(p + c * cstride);
             float tv[CW];
             smem_vec<float, CW>(ts + c * K + g * CW, tv);
+            if constexpr (std::is_same<TL, uint8_t>::value) {
 #pragma unroll
-            for (int k = 0; k < CW; ++k) acc[c] += tof(d.v[k]) * tv[k];
+                for (int k = 0; k < 4; ++k) {
+                    acc[c] += i8_at<0>(d.w[k]) * tv[4 * k];
+                    acc[c] += i8_at<1>(d.w[k]) * tv[4 * k + 1];
+                    acc[c] += i8_at<2>(d.w[k]) * tv[4 * k + 2];
+                    acc[c] += i8_at<3>(d.w[k]) * tv[4 * k + 3];
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < CW; ++k) acc[c] += tof(d.v[k]) * tv[k];
+            }
         }
         p += gstride;
     }
 }
 
 __device__ __forceinline__ void u_task_mixed(const UTaskM &T, const float *__restrict__ U32,
-                                             const __half *__restrict__ U16, const int8_t *__restrict__ U8,
+                                             const __half *__restrict__ U16, const uint8_t *__restrict__ U8,
                                              const float *__restrict__ tpart, const float *__restrict__ scales,
                                              float *__restrict__ slots, float *ts)
 {
@@ -444,7 +471,7 @@ __device__ __forceinline__ void u_task_mixed(const UTaskM &T, const float *__res
         float acc[3] = {0.f, 0.f, 0.f};
         if (T.K[0]) u_row_class<float>(U32 + T.off[0], T.m, r, T.K[0], ts, acc);
         if (T.K[1]) u_row_class<__half>(U16 + T.off[1], T.m, r, T.K[1], ts + base1, acc);
-        if (T.K[2]) u_row_class<int8_t>(U8 + T.off[2], T.m, r, T.K[2], ts + base2, acc);
+        if (T.K[2]) u_row_class<uint8_t>(U8 + T.off[2], T.m, r, T.K[2], ts + base2, acc);
 #pragma unroll
         for (int c = 0; c < 3; ++c) slots[3 * ((int64_t)T.slot + r) + c] = acc[c];
     }
@@ -453,7 +480,7 @@ __device__ __forceinline__ void u_task_mixed(const UTaskM &T, const float *__res
 // V items of all three classes, one warp each (the class picks the element type).
 __global__ void __launch_bounds__(256)
 k_v_mixed(const VItem *__restrict__ vitems, int64_t n_vitems, const float *__restrict__ V32,
-          const __half *__restrict__ V16, const int8_t *__restrict__ V8, const float *__restrict__ x, int xstride,
+          const __half *__restrict__ V16, const uint8_t *__restrict__ V8, const float *__restrict__ x, int xstride,
           float *__restrict__ tpart)
 {
     asm volatile("griddepcontrol.launch_dependents;");
@@ -463,7 +490,7 @@ k_v_mixed(const VItem *__restrict__ vitems, int64_t n_vitems, const float *__res
     const int cls = it.s >> 8, slip = it.s & 255;
     if (cls == 0) v_item<float, float>(it, slip, V32, x, xstride, tpart);
     else if (cls == 1) v_item<__half, float>(it, slip, V16, x, xstride, tpart);
-    else v_item<int8_t, float>(it, slip, V8, x, xstride, tpart);
+    else v_item<uint8_t, float>(it, slip, V8, x, xstride, tpart);
 }
 
 // Dense items, then the mixed U tasks (programmatic dependent launch after k_v_mixed,
@@ -471,7 +498,7 @@ k_v_mixed(const VItem *__restrict__ vitems, int64_t n_vitems, const float *__res
 __global__ void __launch_bounds__(256)
 k_du_mixed(const DenseItem *__restrict__ ditems, int64_t n_ditems, int64_t n_dblocks,
            const UTaskM *__restrict__ tasks, const float *__restrict__ D, const float *__restrict__ U32,
-           const __half *__restrict__ U16, const int8_t *__restrict__ U8, const float *__restrict__ x,
+           const __half *__restrict__ U16, const uint8_t *__restrict__ U8, const float *__restrict__ x,
            float *__restrict__ slots, const float *__restrict__ tpart, const float *__restrict__ scales)
 {
     if (blockIdx.x < n_dblocks) {
@@ -625,7 +652,7 @@ static int run_matvec_mixed(const HmPlan &P, const float *x, float *slots, float
     if (P.n_vitems > 0) {
         const int64_t blocks = (P.n_vitems * 32 + 255) / 256;
         k_v_mixed<<<(unsigned)blocks, 256, 0, st>>>((const VItem *)P.vitems, P.n_vitems, (const float *)P.V,
-                                                    (const __half *)P.V16, (const int8_t *)P.V8, x, x_stride(P.n),
+                                                    (const __half *)P.V16, (const uint8_t *)P.V8, x, x_stride(P.n),
                                                     tpart);
     }
     const int64_t n_dblocks = (P.n_ditems * 32 + 255) / 256;
@@ -647,7 +674,7 @@ static int run_matvec_mixed(const HmPlan &P, const float *x, float *slots, float
         cfg.numAttrs = P.n_vitems > 0 ? 1 : 0;
         PQ3D_CHECK(cudaLaunchKernelEx(&cfg, k_du_mixed, (const DenseItem *)P.ditems, P.n_ditems, n_dblocks,
                                       (const UTaskM *)P.utasks, (const float *)P.dense, (const float *)P.U,
-                                      (const __half *)P.U16, (const int8_t *)P.U8, x, slots, (const float *)tpart,
+                                      (const __half *)P.U16, (const uint8_t *)P.U8, x, slots, (const float *)tpart,
                                       P.scales));
     }
     if (y)

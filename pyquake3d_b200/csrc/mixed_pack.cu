@@ -15,7 +15,8 @@
 //
 //   k_nearfield_rowabs   R3[c][i] += sum_j |K^c_ij| over the dense blocks
 //   k_term_weights       w per (task, term): max over the three components
-//   k_pack_mixed         normalised, quantised factors and per-row scales
+//   k_pack_mixed         normalised, quantised factors and per-row scales; an INT8
+//                        entry b = round(127 v / max|v|) is stored as the byte b + 128
 #include "pq3d_common.cuh"
 #include "hm_layout.cuh"
 #include <cuda_fp16.h>
@@ -127,8 +128,8 @@ __global__ void k_term_weights(const PackTaskM *__restrict__ tasks, const double
 __global__ void k_pack_mixed(const PackTaskM *__restrict__ tasks, const double *__restrict__ ws,
                              const int32_t *__restrict__ rowlist, const int32_t *__restrict__ collist,
                              const int32_t *__restrict__ iperm, const int32_t *__restrict__ tmap,
-                             float *__restrict__ U32, __half *__restrict__ U16, int8_t *__restrict__ U8,
-                             float *__restrict__ V32, __half *__restrict__ V16, int8_t *__restrict__ V8,
+                             float *__restrict__ U32, __half *__restrict__ U16, uint8_t *__restrict__ U8,
+                             float *__restrict__ V32, __half *__restrict__ V16, uint8_t *__restrict__ V8,
                              float *__restrict__ scales)
 {
     __shared__ double red[32];
@@ -168,11 +169,11 @@ __global__ void k_pack_mixed(const PackTaskM *__restrict__ tasks, const double *
             } else {
                 for (int i = threadIdx.x; i < P.m; i += blockDim.x) {
                     const double t = fmin(127.0, fmax(-127.0, rint(127.0 * u[i] / su)));
-                    U8[P.u_off[2] + u_index(P.m, iperm[rows[i]] - P.r0, c, col, 16)] = (int8_t)t;
+                    U8[P.u_off[2] + u_index(P.m, iperm[rows[i]] - P.r0, c, col, 16)] = (uint8_t)(t + 128.0);
                 }
                 for (int j = threadIdx.x; j < P.n; j += blockDim.x) {
                     const double t = fmin(127.0, fmax(-127.0, rint(127.0 * v[j] / sv)));
-                    V8[P.v_off[2] + v_index(P.Q[2], row, P.c0 % 16 + iperm[cols[j]] - P.c0, 16)] = (int8_t)t;
+                    V8[P.v_off[2] + v_index(P.Q[2], row, P.c0 % 16 + iperm[cols[j]] - P.c0, 16)] = (uint8_t)(t + 128.0);
                 }
                 if (threadIdx.x == 0) scales[P.sb[2] + row] = (float)(su * sv / (127.0 * 127.0));
             }
@@ -224,8 +225,8 @@ PQ3D_EXPORT int pq3d_aca_pack_mixed(const void *d_tasks, int64_t n_tasks, const 
     for (int64_t t0 = 0; t0 < n_tasks; t0 += 65535) {
         const unsigned nt = (unsigned)(n_tasks - t0 < 65535 ? n_tasks - t0 : 65535);
         k_pack_mixed<<<nt, 256, 0, stream>>>((const PackTaskM *)d_tasks + t0, d_ws, d_rowlist, d_collist, d_iperm,
-                                             d_tmap, d_U32, (__half *)d_U16, (int8_t *)d_U8, d_V32, (__half *)d_V16,
-                                             (int8_t *)d_V8, d_scales);
+                                             d_tmap, d_U32, (__half *)d_U16, (uint8_t *)d_U8, d_V32, (__half *)d_V16,
+                                             (uint8_t *)d_V8, d_scales);
     }
     return pq3d_launch_status();
 }

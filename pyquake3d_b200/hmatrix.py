@@ -17,6 +17,7 @@ with the FP64 Green's function, admissible blocks with batched ACA), packs it
 for one or more storage precisions and applies it with pq3d_hmatvec.
 """
 import math
+import os
 
 import numpy as np
 
@@ -433,6 +434,25 @@ def _rec(rows, dt):
     return np.array(rows, dtype=dt) if rows else np.zeros(1, dtype=dt)
 
 
+# ----------------------------------------------------------------------------- plan cache
+
+PLAN_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "plan_cache.json")
+_plan_cache = None
+
+
+def plan_cache_entry(gpu_name, dtype):
+    """Work-item shapes measured by pyquake3d_b200.autotune for this GPU model and
+    storage, or None."""
+    global _plan_cache
+    if _plan_cache is None:
+        _plan_cache = {}
+        if os.path.exists(PLAN_CACHE):
+            import json
+            with open(PLAN_CACHE) as f:
+                _plan_cache = json.load(f)
+    return _plan_cache.get(gpu_name, {}).get(dtype)
+
+
 # ----------------------------------------------------------------------------- device operator
 
 DTYPES = {"fp64": 0, "fp32": 1, "bf16": 2, "mixed": 3}
@@ -455,10 +475,12 @@ class DeviceHMatrix:
     ("fp64": FP64 everywhere; "fp32": FP32 everywhere; "bf16": FP32 dense,
     BF16 low rank).  matvec(x_dev, dtype) returns y (n x 3, FP64, tree order)."""
 
-    # work-item shapes per storage code (0 FP64, 1 FP32, 2 BF16 low rank), tuned on B200 at 60k
-    DENSE_CHUNK_GROUPS = {0: 64, 1: 16, 2: 16}   # column groups per dense work item
-    V_CHUNK_GROUPS = {0: 128, 1: 32, 2: 32}      # column groups per V work item
-    U_ROWS = 512                                 # rows per U task (one CTA)
+    # work-item shapes per storage code (0 FP64, 1 FP32, 2 BF16 low rank, 3 mixed): these
+    # defaults unless the plan cache written by pyquake3d_b200.autotune has an entry for
+    # this GPU and storage (shapes()).
+    DENSE_CHUNK_GROUPS = {0: 64, 1: 16, 2: 16, 3: 16}   # column groups per dense work item
+    V_CHUNK_GROUPS = {0: 128, 1: 32, 2: 32, 3: 32}      # column groups per V work item
+    U_ROWS = 512                                        # rows per U task (one CTA)
 
     def __init__(self, struct, xg, ev, nodes, tri, mu, lam, device="cuda", aca_tol=0.01, aca_rel=False,
                  aca_seed=0, kcap=96, ws_budget_bytes=8 << 30, keep_factors=False, halfspace=0,
@@ -468,6 +490,7 @@ class DeviceHMatrix:
         compiled library (the values its H-matrix assembly uses).  mixed_tol: the
         term-class tolerance of the "mixed" storage (classify_terms)."""
         self.mixed_tol = float(mixed_tol)
+        self.use_plan_cache = True
         import torch
         self.torch = torch
         self.L = _lib.load()
@@ -671,14 +694,47 @@ class DeviceHMatrix:
                   "pq3d_aca_pack")
         return self._finish_plan(dtype, A, Ubuf, Vbuf)
 
+    def shapes(self, dtype):
+        """(dense_chunk, v_chunk, u_rows) of a storage: an explicit override
+        (set_shapes), else the plan cache's entry for this GPU, else the defaults."""
+        code = DTYPES[dtype]
+        ov = getattr(self, "_shape_override", {}).get(dtype)
+        if ov is not None:
+            return ov
+        if self.use_plan_cache:
+            ent = plan_cache_entry(self.torch.cuda.get_device_name(self.dev), dtype)
+            if ent is not None:
+                return int(ent["dense_chunk"]), int(ent["v_chunk"]), int(ent["u_rows"])
+        return self.DENSE_CHUNK_GROUPS[code], self.V_CHUNK_GROUPS[code], self.U_ROWS
+
+    def set_shapes(self, dtype, dense_chunk, v_chunk, u_rows):
+        """Rebuild one storage's work items with other shapes; the packed operator data
+        does not depend on them and is kept (the autotuner's move)."""
+        if not hasattr(self, "_shape_override"):
+            self._shape_override = {}
+        self._shape_override[dtype] = (int(dense_chunk), int(v_chunk), int(u_rows))
+        P = self.plans.get(dtype)
+        if P is None:
+            return None
+        if DTYPES[dtype] == 3:
+            offs = np.concatenate([[0], np.cumsum(np.asarray(self.aca_ranks, np.int64))])
+            t = self.mixed_tmap
+            cls_lists = [(t[offs[2 * bi]:offs[2 * bi + 1]] & 3, t[offs[2 * bi + 1]:offs[2 * bi + 2]] & 3)
+                         for bi in range(len(self.aca_blocks))]
+            A = self._mixed_arrays(cls_lists)
+            A["mixed"] = P["mixed"]
+        else:
+            A = self.plan_arrays(dtype)
+        del self.plans[dtype]
+        return self._finish_plan(dtype, A, P["U"], P["V"])
+
     def plan_arrays(self, dtype):
         """Host work-item arrays of one storage precision (deterministic from the
         structure and the ACA ranks)."""
         code = DTYPES[dtype]
         kS, kD = self.ranks()
-        pick = lambda v: v[code] if isinstance(v, dict) else v
-        return build_plan_arrays(self.s, self.dense_recs, kS, kD, code, pick(self.DENSE_CHUNK_GROUPS),
-                                 pick(self.V_CHUNK_GROUPS), self.U_ROWS)
+        dc, vc, ur = self.shapes(dtype)
+        return build_plan_arrays(self.s, self.dense_recs, kS, kD, code, dc, vc, ur)
 
     def _task_records_mixed(self, keep_ws):
         """PackTaskM records (per workspace batch) for every ACA task, with the weight /
@@ -741,9 +797,11 @@ class DeviceHMatrix:
                 tmap[offs[ti]:offs[ti + 1]] = cc | (pos << 2)
         self.mixed_tmap = tmap[:int(offs[-1])]
         A = self._mixed_arrays(cls_lists)
-        tdt = (torch.float32, torch.float16, torch.int8)
-        Ub = [torch.zeros(max(int(A["u_sizes"][c]), 16), dtype=tdt[c], device=self.dev) for c in range(3)]
-        Vb = [torch.zeros(max(int(A["v_sizes"][c]), 16), dtype=tdt[c], device=self.dev) for c in range(3)]
+        # INT8-class entries are stored as b + 128: the fill 128 decodes to zero, so padding
+        # columns (a block's lead and tail columns, its K padding) contribute nothing
+        tdt, fill = (torch.float32, torch.float16, torch.uint8), (0, 0, 128)
+        Ub = [torch.full((max(int(A["u_sizes"][c]), 16),), fill[c], dtype=tdt[c], device=self.dev) for c in range(3)]
+        Vb = [torch.full((max(int(A["v_sizes"][c]), 16),), fill[c], dtype=tdt[c], device=self.dev) for c in range(3)]
         scales = torch.zeros(max(A["n_scales"], 4), dtype=torch.float32, device=self.dev)
         d_tmap = torch.from_numpy(tmap).to(self.dev)
         layout = {}
@@ -770,8 +828,8 @@ class DeviceHMatrix:
         return self._finish_plan("mixed", A, Ub[0], Vb[0])
 
     def _mixed_arrays(self, cls_lists):
-        return build_plan_arrays_mixed(self.s, self.dense_recs, cls_lists, self.DENSE_CHUNK_GROUPS[1],
-                                       self.V_CHUNK_GROUPS[1], self.U_ROWS)
+        dc, vc, ur = self.shapes("mixed")
+        return build_plan_arrays_mixed(self.s, self.dense_recs, cls_lists, dc, vc, ur)
 
     def install_mixed(self, tmap, U, V, scales):
         """Register a mixed plan whose class arrays come from elsewhere (an operator

@@ -584,6 +584,7 @@ class DeviceStepper:
         self.args["fix_tn"] = self.fix_tn
         self.args["x_fp32"] = 0 if self.x.dtype == torch.float64 else 1
         P = op.plan(precision)
+        self._plan = P                  # the plan whose buffers args points into
         self.args["slots"] = P["slots"].data_ptr()
         self.args["leaf_of_row"] = P["leaf_of_row"].data_ptr()
         self.args["leaf_ptr"] = P["leaf_ptr"].data_ptr()
@@ -603,6 +604,9 @@ class DeviceStepper:
 
     def _rk(self, step_index, h_in, stream=None, ctrl_host=0):
         """Enqueue the step kernel alone (the slots must hold the products of x)."""
+        if self.op.plans.get(self.precision) is not self._plan:
+            raise _lib.Pq3dError("the operator's work items were rebuilt after this stepper was created; "
+                                 "create a new stepper")
         self._state_event = False
         self._prefetched = None
         self.version += 1

@@ -6,7 +6,9 @@ packed with the index formulas of the CUDA kernels (mixed_pack.cu:
 k_nearfield_rowabs, k_term_weights, k_pack_mixed; hm_layout.cuh u_index /
 v_index with column groups 4, 8, 16); every packed index is checked against
 the array sizes build_plan_arrays_mixed gives, and the work items are executed
-by numpy emulations of k_v_mixed, k_du_mixed and k_rowsum.  The products must
+by numpy emulations of k_v_mixed, k_du_mixed and k_rowsum (INT8 entries are
+stored as the byte b + 128 and the arrays filled with 128, which decodes to
+zero in padding).  The products must
 stay within the classification's error bound of the oracle's FP64
 blocks_process_MVM products: every row within a small multiple of
 tol * R_i * max|x| (R_i the near-field absolute row sum the weights use), and
@@ -92,9 +94,9 @@ def pack_mixed(st, op, tol):
     W = _weights(st, op, R)
     cls_lists = [classify_terms(wS, wD, tol) for wS, wD in W]
     A = build_plan_arrays_mixed(st, recs, cls_lists, dense_chunk=2, v_chunk=3, u_rows=40)
-    dt = (np.float32, np.float16, np.int8)
-    U = [np.zeros(max(A["u_sizes"][c], 16), dt[c]) for c in range(3)]
-    V = [np.zeros(max(A["v_sizes"][c], 16), dt[c]) for c in range(3)]
+    dt, fill = (np.float32, np.float16, np.uint8), (0, 0, 128)      # INT8 entries stored as b + 128
+    U = [np.full(max(A["u_sizes"][c], 16), fill[c], dt[c]) for c in range(3)]
+    V = [np.full(max(A["v_sizes"][c], 16), fill[c], dt[c]) for c in range(3)]
     scales = np.zeros(max(A["n_scales"], 4), np.float32)
     layout = {(bi, p): (uo, vo, ks, kd, Q, K, sb) for (bi, p, uo, vo, ks, kd, Q, K, sb) in A["pack"]}
     ab, oa = [b for b in st.blocks if b.aca], [b for b in op.blocks if b[0] == "aca"]
@@ -134,10 +136,15 @@ def pack_mixed(st, op, tol):
                         V[1][iv] = (v / sv).astype(np.float32).astype(np.float16)
                         scales[sb[1] + row] = np.float32(su * sv)
                     else:
-                        U[2][iu] = np.clip(np.rint(127 * u / su), -127, 127).astype(np.int8)
-                        V[2][iv] = np.clip(np.rint(127 * v / sv), -127, 127).astype(np.int8)
+                        U[2][iu] = (np.clip(np.rint(127 * u / su), -127, 127) + 128).astype(np.uint8)
+                        V[2][iv] = (np.clip(np.rint(127 * v / sv), -127, 127) + 128).astype(np.uint8)
                         scales[sb[2] + row] = np.float32(su * sv / 127.0 ** 2)
     return A, D, U, V, scales, R, cls_lists
+
+
+def _decode(a, cls):
+    """Stored class entries as float64 (INT8 bytes hold b + 128)."""
+    return a.astype(np.float64) - 128.0 if cls == 2 else a.astype(np.float64)
 
 
 def emulate(st, A, D, U, V, scales, x):
@@ -164,7 +171,7 @@ def emulate(st, A, D, U, V, scales, x):
             for g in range(int(it["g0"]), int(it["g1"])):
                 idx = it["off"] + (g * Q + q) * cw + np.arange(cw)
                 assert idx.max() < len(V[cls])
-                acc += float(np.dot(V[cls][idx].astype(np.float64),
+                acc += float(np.dot(_decode(V[cls][idx], cls),
                                     x[(2 + slip) * x_stride(st.n) + int(it["c0"]) + g * cw + np.arange(cw)]))
             tpart[int(it["tp"]) + q] = acc
     for T in A["utasks"][:A["n_utasks"]]:
@@ -187,7 +194,7 @@ def emulate(st, A, D, U, V, scales, x):
                     for k in range(cw):
                         idx = T["off"][cls] + ((g * 3 + c) * m + rr) * cw + k
                         assert idx.max() < len(U[cls])
-                        acc[:, c] += U[cls][idx].astype(np.float64) * tv[c * K + g * cw + k]
+                        acc[:, c] += _decode(U[cls][idx], cls) * tv[c * K + g * cw + k]
         slots[3 * (int(T["slot"]) + rr)[:, None] + np.arange(3)] = acc
     y = np.zeros((st.n, 3))
     for i in range(st.n):
