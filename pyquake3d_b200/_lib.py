@@ -29,7 +29,10 @@ _PLAN_PTRS = ["dense", "U", "V", "ditems", "vitems", "utasks", "leaf_of_row", "l
 HM_PLAN = np.dtype([("n", "i4"), ("dtype", "i4")] + [(p, "u8") for p in _PLAN_PTRS] +
                    [(k, "i8") for k in ("n_ditems", "n_vitems", "n_utasks", "n_slots", "n_tpart")] +
                    [("kmax", "i4"), ("pad", "i4")] +
-                   [(p, "u8") for p in ("U16", "V16", "U8", "V8", "scales")], align=True)
+                   [(p, "u8") for p in ("U16", "V16", "U8", "V8", "scales", "status")] +
+                   [("stream", "i4"), ("pad2", "i4")], align=True)
+# streamed mixed kernels (hmatvec.cu): stage size, x-slice width and rows per U task
+STREAM_STAGE_BYTES, STREAM_XMAX, STREAM_ROWS = 12288, 1024, 256
 # mixed storage (FP32 / FP16 / INT8 term classes): U task and packing records
 U_TASK_M = np.dtype([("off", "i8", 3), ("m", "i4"), ("r0", "i4"), ("r1", "i4"), ("slot", "i4")] +
                     [(k, "i4", 3) for k in ("K", "kS", "kD", "Q", "tp", "nch", "sb")] + [("pad", "i4")], align=True)

@@ -512,6 +512,324 @@ k_du_mixed(const DenseItem *__restrict__ ditems, int64_t n_ditems, int64_t n_dbl
     u_task_mixed(T, U32, U16, U8, tpart, scales, slots, reinterpret_cast<float *>(smraw));
 }
 
+// ------------------------------------------------------------------ mixed storage, streamed
+// The same products as k_v_mixed / k_du_mixed, with the low-rank factors moved by
+// bulk copies: every task reads contiguous runs of the packed operator, so one
+// producer warp streams them into a ring of ST_STAGES shared-memory stages with
+// 1-D cp.async.bulk (global -> shared, completion counted in bytes on the stage's
+// "full" mbarrier) while eight consumer warps compute from shared memory and
+// release the stage on its "empty" mbarrier.  The loads no longer wait in
+// registers: a CTA keeps up to ST_STAGES * ST_STAGE_BYTES in flight.
+//   V task (VItem with q = 0, nr = Q, s = 3 kS | cls << 16): all Q rows of one
+//     class of one block over column groups [g0, g1) -- one contiguous range of
+//     (g1 - g0) Q 16-byte units; its x slices (strike and dip planes) sit in
+//     shared memory.  Threads map to (row, group residue) pairs; each group's
+//     partials are reduced across the residues at the end.
+//   U task (UTaskM, r1 - r0 <= ST_CONSUMERS): per class and column group, the
+//     three components' runs of rows [r0, r1) (three copies into one stage);
+//     one consumer thread per row.
+// All waits are bounded (ST_SPIN polls); a timeout stores 1 in *status, and the
+// producer still waits, bounded, for the copies it issued before the CTA exits.
+constexpr int ST_STAGES = 4;
+constexpr int ST_STAGE_BYTES = 12288;
+constexpr int ST_CONSUMERS = 256;
+constexpr int ST_THREADS = ST_CONSUMERS + 32;
+constexpr int ST_XMAX = 1024;             // columns of a V task's x slices
+constexpr long long ST_SPIN = 1ll << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *b, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, unsigned bytes)
+{
+    uint64_t st;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+                 : "=l"(st) : "r"(smem_addr(b)), "r"(bytes) : "memory");
+    (void)st;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *b)
+{
+    uint64_t st;
+    asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];" : "=l"(st) : "r"(smem_addr(b)) : "memory");
+    (void)st;
+}
+// Bounded wait for the phase of parity `parity` to complete; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity)
+{
+    const uint32_t a = smem_addr(b);
+    for (long long i = 0; i < ST_SPIN; ++i) {
+        uint32_t ok;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(ok) : "r"(a), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+// 1-D bulk copy global -> this CTA's shared memory; completion counted on `bar`.
+// dst, src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, %0;" ::"n"(ST_CONSUMERS) : "memory"); }
+
+__device__ __forceinline__ void st_init_barriers(uint64_t *full, uint64_t *empty)
+{
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < ST_STAGES; ++s) {
+            mbar_init(full + s, 1);                     // the producer's arrive.expect_tx
+            mbar_init(empty + s, ST_CONSUMERS / 32);    // one arrive per consumer warp
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+}
+
+// Producer epilogue: bounded wait for the copies of the last pieces it issued.
+__device__ __forceinline__ void st_drain(uint64_t *full, int issued, int *status)
+{
+    for (int i = issued > ST_STAGES ? issued - ST_STAGES : 0; i < issued; ++i)
+        if (!mbar_wait(full + i % ST_STAGES, (unsigned)(i / ST_STAGES) & 1u)) atomicExch(status, 1);
+}
+
+// dot of one 16-byte unit of class element type TL with CW floats of x (or t)
+template <typename TL>
+__device__ __forceinline__ float dot16(const unsigned char *u, const float *xv)
+{
+    const int4 r = *reinterpret_cast<const int4 *>(u);
+    Vec16<TL> d;
+    memcpy(&d, &r, 16);
+    float a = 0.f;
+    if constexpr (std::is_same<TL, uint8_t>::value) {
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            a += i8_at<0>(d.w[t]) * xv[4 * t];
+            a += i8_at<1>(d.w[t]) * xv[4 * t + 1];
+            a += i8_at<2>(d.w[t]) * xv[4 * t + 2];
+            a += i8_at<3>(d.w[t]) * xv[4 * t + 3];
+        }
+    } else {
+        constexpr int CW = 16 / sizeof(TL);
+#pragma unroll
+        for (int t = 0; t < CW; ++t) a += tof(d.v[t]) * xv[t];
+    }
+    return a;
+}
+
+template <typename TL>
+__device__ void v_task_stream(const VItem &T, const TL *__restrict__ Vc, const float *__restrict__ x, int xstride,
+                              float *__restrict__ tpart, unsigned char *stage, uint64_t *full, uint64_t *empty,
+                              float *xs, float *red, int *status)
+{
+    constexpr int CW = 16 / sizeof(TL);
+    const int Q = T.Q, G = T.g1 - T.g0, kS3 = T.s & 0xffff;
+    // sizes the plan builder never produces: reject before any barrier or copy
+    if (Q <= 0 || Q * 16 > ST_STAGE_BYTES || G <= 0 || G * CW > ST_XMAX) {
+        if (threadIdx.x == 0) atomicExch(status, 2);
+        return;
+    }
+    const int gp = ST_STAGE_BYTES / (Q * 16);                        // whole groups per piece (>= 1)
+    const int npieces = (G + gp - 1) / gp;
+    const unsigned char *src = reinterpret_cast<const unsigned char *>(Vc + T.off) + (int64_t)T.g0 * Q * 16;
+    const int tid = threadIdx.x;
+    if (tid >= ST_CONSUMERS) {                                       // producer warp
+        if (tid == ST_CONSUMERS) {
+            int i = 0;
+            for (; i < npieces; ++i) {
+                const int s = i % ST_STAGES;
+                if (i >= ST_STAGES && !mbar_wait(empty + s, (unsigned)(i / ST_STAGES - 1) & 1u)) {
+                    atomicExch(status, 1);
+                    break;
+                }
+                const int ga = i * gp, ng = min(gp, G - ga);
+                const unsigned nb = (unsigned)(ng * Q * 16);
+                mbar_expect_tx(full + s, nb);
+                bulk_g2s(stage + (size_t)s * ST_STAGE_BYTES, src + (int64_t)ga * Q * 16, nb, full + s);
+            }
+            st_drain(full, i, status);
+        }
+        return;
+    }
+    // x slices of the task's columns (strike and dip planes)
+    const float *xg = x + T.c0 + (int64_t)T.g0 * CW;
+    for (int c = tid; c < G * CW; c += ST_CONSUMERS) {
+        xs[c] = xg[2 * (int64_t)xstride + c];
+        xs[ST_XMAX + c] = xg[3 * (int64_t)xstride + c];
+    }
+    consumers_sync();
+    // thread -> (row q, group residue r): R residues when Q <= 256, else rows tid, tid + 256, ...
+    const int R = Q <= ST_CONSUMERS ? ST_CONSUMERS / Q : 1;
+    const bool act = tid < R * Q || Q > ST_CONSUMERS;
+    const int q0 = Q <= ST_CONSUMERS ? tid % Q : tid, r = Q <= ST_CONSUMERS ? tid / Q : 0;
+    float acc[3] = {0.f, 0.f, 0.f};
+    for (int i = 0; i < npieces; ++i) {
+        const int s = i % ST_STAGES;
+        const bool ok = mbar_wait(full + s, (unsigned)(i / ST_STAGES) & 1u);
+        if (!ok) atomicExch(status, 1);
+        if (ok && act) {
+            const unsigned char *st = stage + (size_t)s * ST_STAGE_BYTES;
+            const int ga = i * gp, gb = min(G, ga + gp);
+            for (int g = ga + r; g < gb; g += R) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const int q = q0 + k * ST_CONSUMERS;
+                    if (q < Q && (k == 0 || Q > ST_CONSUMERS))
+                        acc[k] += dot16<TL>(st + ((size_t)(g - ga) * Q + q) * 16, xs + (q < kS3 ? 0 : ST_XMAX) + g * CW);
+                }
+            }
+        }
+        __syncwarp();
+        if ((tid & 31) == 0) mbar_arrive(empty + s);
+    }
+    if (Q <= ST_CONSUMERS) {
+        red[tid] = act ? acc[0] : 0.f;
+        consumers_sync();
+        if (tid < Q) {
+            float v = 0.f;
+            for (int rr = 0; rr < R; ++rr) v += red[rr * Q + tid];
+            tpart[T.tp + tid] = v;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (q0 + k * ST_CONSUMERS < Q) tpart[T.tp + q0 + k * ST_CONSUMERS] = acc[k];
+    }
+}
+
+__global__ void __launch_bounds__(ST_THREADS, 1)
+k_v_stream(const VItem *__restrict__ tasks, const float *__restrict__ V32, const __half *__restrict__ V16,
+           const uint8_t *__restrict__ V8, const float *__restrict__ x, int xstride, float *__restrict__ tpart,
+           int *status)
+{
+    asm volatile("griddepcontrol.launch_dependents;");
+    extern __shared__ __align__(128) unsigned char sm[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(sm), *empty = full + ST_STAGES;
+    float *xs = reinterpret_cast<float *>(sm + 128);
+    float *red = xs + 2 * ST_XMAX;
+    unsigned char *stage = sm + 128 + (2 * ST_XMAX + ST_CONSUMERS) * 4;
+    st_init_barriers(full, empty);
+    const VItem T = tasks[blockIdx.x];
+    const int cls = T.s >> 16;
+    if (cls == 0) v_task_stream<float>(T, V32, x, xstride, tpart, stage, full, empty, xs, red, status);
+    else if (cls == 1) v_task_stream<__half>(T, V16, x, xstride, tpart, stage, full, empty, xs, red, status);
+    else v_task_stream<uint8_t>(T, V8, x, xstride, tpart, stage, full, empty, xs, red, status);
+}
+
+// Dense items (nine warps per CTA), then U tasks with bulk-copied factors.  The
+// producer starts streaming U right away (it does not depend on k_v_stream); the
+// consumers wait for k_v_stream (griddepcontrol.wait) before gathering t.
+__global__ void __launch_bounds__(ST_THREADS, 1)
+k_du_stream(const DenseItem *__restrict__ ditems, int64_t n_ditems, int64_t n_dblocks,
+            const UTaskM *__restrict__ tasks, const float *__restrict__ D, const float *__restrict__ U32,
+            const __half *__restrict__ U16, const uint8_t *__restrict__ U8, const float *__restrict__ x,
+            float *__restrict__ slots, const float *__restrict__ tpart, const float *__restrict__ scales,
+            int *status)
+{
+    if (blockIdx.x < n_dblocks) {
+        const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+        dense_v_item<float, float, float>(w, ditems, n_ditems, nullptr, 0, D, nullptr, x, 0, slots, nullptr);
+        return;
+    }
+    extern __shared__ __align__(128) unsigned char sm[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(sm), *empty = full + ST_STAGES;
+    unsigned char *stage = sm + 128;
+    float *ts = reinterpret_cast<float *>(stage + (size_t)ST_STAGES * ST_STAGE_BYTES);
+    st_init_barriers(full, empty);
+    const UTaskM T = tasks[blockIdx.x - n_dblocks];
+    const int rows = T.r1 - T.r0;
+    if (rows <= 0 || rows > ST_CONSUMERS) {                          // the plan builder never produces these
+        if (threadIdx.x == 0) atomicExch(status, 2);
+        return;
+    }
+    const int ng0 = T.K[0] / 4, ng1 = T.K[1] / 8, ng2 = T.K[2] / 16;
+    const int tid = threadIdx.x;
+    const unsigned run = (unsigned)rows * 16u;                       // bytes of one component's rows
+    if (tid >= ST_CONSUMERS) {                                       // producer warp
+        if (tid == ST_CONSUMERS) {
+            int i = 0;
+            bool stop = false;
+#pragma unroll 1
+            for (int cls = 0; cls < 3 && !stop; ++cls) {
+                const unsigned char *base =
+                    cls == 0 ? reinterpret_cast<const unsigned char *>(U32 + T.off[0])
+                             : (cls == 1 ? reinterpret_cast<const unsigned char *>(U16 + T.off[1])
+                                         : reinterpret_cast<const unsigned char *>(U8 + T.off[2]));
+                const int ngc = cls == 0 ? ng0 : (cls == 1 ? ng1 : ng2);
+                for (int g = 0; g < ngc; ++g, ++i) {
+                    const int s = i % ST_STAGES;
+                    if (i >= ST_STAGES && !mbar_wait(empty + s, (unsigned)(i / ST_STAGES - 1) & 1u)) {
+                        atomicExch(status, 1);
+                        stop = true;
+                        break;
+                    }
+                    mbar_expect_tx(full + s, 3 * run);
+                    unsigned char *dst = stage + (size_t)s * ST_STAGE_BYTES;
+                    for (int c = 0; c < 3; ++c)
+                        bulk_g2s(dst + c * run, base + (((int64_t)g * 3 + c) * T.m + T.r0) * 16, run, full + s);
+                }
+            }
+            st_drain(full, i, status);
+        }
+        return;
+    }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    // t of every class (scaled), as u_task_mixed
+    const int base1 = 3 * T.K[0], base2 = 3 * (T.K[0] + T.K[1]);
+#pragma unroll
+    for (int cls = 0; cls < 3; ++cls) {
+        const int K = T.K[cls], kS = T.kS[cls], kD = T.kD[cls];
+        float *tc = ts + (cls == 0 ? 0 : (cls == 1 ? base1 : base2));
+        for (int e = tid; e < 3 * K; e += ST_CONSUMERS) {
+            const int c = e / K, q = e % K;
+            int row = -1;
+            if (q < kS) row = c * kS + q;
+            else if (q < kS + kD) row = 3 * kS + c * kD + (q - kS);
+            float v = 0.f;
+            if (row >= 0) {
+                v = sum_partials<float>(tpart + T.tp[cls] + row, T.nch[cls], T.Q[cls]);
+                if (cls > 0) v *= scales[T.sb[cls] + row];
+            }
+            tc[e] = v;
+        }
+    }
+    consumers_sync();
+    float acc[3] = {0.f, 0.f, 0.f};
+    const bool act = tid < rows;
+    int i = 0;
+#pragma unroll 1
+    for (int cls = 0; cls < 3; ++cls) {
+        const int K = cls == 0 ? T.K[0] : (cls == 1 ? T.K[1] : T.K[2]);
+        const int ngc = cls == 0 ? ng0 : (cls == 1 ? ng1 : ng2);
+        const float *tc = ts + (cls == 0 ? 0 : (cls == 1 ? base1 : base2));
+        for (int g = 0; g < ngc; ++g, ++i) {
+            const int s = i % ST_STAGES;
+            const bool ok = mbar_wait(full + s, (unsigned)(i / ST_STAGES) & 1u);
+            if (!ok) atomicExch(status, 1);
+            if (ok && act) {
+                const unsigned char *st = stage + (size_t)s * ST_STAGE_BYTES + (size_t)tid * 16;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    if (cls == 0) acc[c] += dot16<float>(st + c * run, tc + c * K + g * 4);
+                    else if (cls == 1) acc[c] += dot16<__half>(st + c * run, tc + c * K + g * 8);
+                    else acc[c] += dot16<uint8_t>(st + c * run, tc + c * K + g * 16);
+                }
+            }
+            __syncwarp();
+            if ((tid & 31) == 0) mbar_arrive(empty + s);
+        }
+    }
+    if (act) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) slots[3 * ((int64_t)T.slot + T.r0 + tid) + c] = acc[c];
+    }
+}
+
 // ------------------------------------------------------------------ kernel 3
 // y[3i+c] = sum of row i's slots (in list order) + add[c][i] (FP64), for rows of leaf clusters.
 template <typename TA>
@@ -575,6 +893,8 @@ struct HmPlan {
     // storage code 3 only (U, V above are the FP32 class arrays)
     const void *U16, *V16, *U8, *V8;   // FP16 and INT8 class arrays
     const float *scales;               // per-V-row scales of the FP16 and INT8 classes
+    int32_t *status;                   // streamed kernels: 1 after a timed-out wait (else untouched)
+    int32_t stream, pad2;              // 1: the low-rank work runs in k_v_stream / k_du_stream
 };
 
 PQ3D_EXPORT size_t pq3d_item_bytes(int kind)
@@ -683,6 +1003,44 @@ static int run_matvec_mixed(const HmPlan &P, const float *x, float *slots, float
     return pq3d_launch_status();
 }
 
+// Storage code 3 with streamed low-rank work (plan.stream = 1).
+static int run_matvec_stream(const HmPlan &P, const float *x, float *slots, float *tpart, const double *add0,
+                             const double *add1, const double *add2, double *y, cudaStream_t st)
+{
+    if (!P.status) return PQ3D_ERR_ARG;
+    const size_t smv = 128 + (2 * ST_XMAX + ST_CONSUMERS) * 4 + (size_t)ST_STAGES * ST_STAGE_BYTES;
+    const size_t smu = 128 + (size_t)ST_STAGES * ST_STAGE_BYTES + (size_t)3 * P.kmax * sizeof(float);
+    if (smu > 200 * 1024) return PQ3D_ERR_ARG;
+    PQ3D_CHECK(cudaFuncSetAttribute(k_v_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smv));
+    PQ3D_CHECK(cudaFuncSetAttribute(k_du_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smu));
+    if (P.n_vitems > 0)
+        k_v_stream<<<(unsigned)P.n_vitems, ST_THREADS, smv, st>>>((const VItem *)P.vitems, (const float *)P.V,
+                                                                  (const __half *)P.V16, (const uint8_t *)P.V8, x,
+                                                                  x_stride(P.n), tpart, P.status);
+    const int64_t n_dblocks = (P.n_ditems * 32 + ST_THREADS - 1) / ST_THREADS;
+    const int64_t grid = n_dblocks + P.n_utasks;
+    if (grid > 0) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)grid);
+        cfg.blockDim = dim3(ST_THREADS);
+        cfg.dynamicSmemBytes = smu;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = P.n_vitems > 0 ? 1 : 0;
+        PQ3D_CHECK(cudaLaunchKernelEx(&cfg, k_du_stream, (const DenseItem *)P.ditems, P.n_ditems, n_dblocks,
+                                      (const UTaskM *)P.utasks, (const float *)P.dense, (const float *)P.U,
+                                      (const __half *)P.U16, (const uint8_t *)P.U8, x, slots, (const float *)tpart,
+                                      P.scales, P.status));
+    }
+    if (y)
+        k_rowsum<float><<<(P.n + 255) / 256, 256, 0, st>>>(P.n, P.leaf_of_row, P.leaf_ptr, P.leaf_off, slots, add0,
+                                                           add1, add2, y);
+    return pq3d_launch_status();
+}
+
 // y (n x 3, FP64, tree order) = K x (+ add_c).  x: deficit in the layout of hm_layout.cuh
 // (4 * x_stride(n) entries: interleaved, strike plane, dip plane), FP64 for dtype 0 and
 // FP32 otherwise.  Scratch: slots (3*n_slots) and
@@ -708,6 +1066,9 @@ PQ3D_EXPORT int pq3d_hmatvec(const void *plan_host, const void *d_x, void *d_slo
                                                        d_add0, d_add1, d_add2, d_y, stream);
     case 3:
         if (P.n_utasks > 0 && (!P.U || !P.U16 || !P.U8 || !P.V || !P.V16 || !P.V8 || !P.scales)) return PQ3D_ERR_ARG;
+        if (P.stream)
+            return run_matvec_stream(P, (const float *)d_x, (float *)d_slots, (float *)d_tpart, d_add0, d_add1,
+                                     d_add2, d_y, stream);
         return run_matvec_mixed(P, (const float *)d_x, (float *)d_slots, (float *)d_tpart, d_add0, d_add1, d_add2,
                                 d_y, stream);
     }

@@ -366,11 +366,18 @@ def classify_terms(wS, wD, tol):
     return cls[:len(wS)], cls[len(wS):]
 
 
-def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chunk=32, u_rows=512):
+def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chunk=32, u_rows=512, stream=False):
     """Work items, slot layout and packing records of the mixed storage (code 3):
     FP32 dense items as in the FP32 plan; per low-rank block and term class c
     (FP32, FP16, INT8) the class's own U / V arrays with column groups MIXED_CW[c].
-    cls_lists[bi] = (cls_S, cls_D) from classify_terms.  Pure numpy."""
+    cls_lists[bi] = (cls_S, cls_D) from classify_terms.  Pure numpy.
+
+    stream=True lays the work out for the bulk-copy kernels (k_v_stream,
+    k_du_stream): one V task per (block, class, column chunk) covering all the
+    class's rows (VItem with q = 0, nr = Q, s = 3 kS | class << 16; chunks of at
+    most STREAM_XMAX columns), and U tasks of at most STREAM_ROWS rows."""
+    if stream:
+        u_rows = min(u_rows, _lib.STREAM_ROWS)
     ditems, slot_rows, slot = _dense_items(dense_recs, 4, dense_recs["off32"], dense_chunk)
     aca_blocks = [b for b in struct.blocks if b.aca]
     u_off, v_off = [0, 0, 0], [0, 0, 0]
@@ -400,9 +407,16 @@ def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chu
                 continue
             lead = b.col.start % cw
             ngv = _cdiv(nn + lead, cw)
-            nch = _cdiv(ngv, v_chunk)
+            gch = min(v_chunk, _lib.STREAM_XMAX // cw) if stream else v_chunk
+            nch = _cdiv(ngv, gch)
+            if stream and Qs[c] * 16 > _lib.STREAM_STAGE_BYTES:
+                raise _lib.Pq3dError("a block's term class has %d V rows, more than one stream stage holds" % Qs[c])
             for ch in range(nch):
-                g0, g1 = ch * v_chunk, min(ngv, (ch + 1) * v_chunk)
+                g0, g1 = ch * gch, min(ngv, (ch + 1) * gch)
+                if stream:
+                    vitems.append((v_off[c], Qs[c], 0, Qs[c], g0, g1, b.col.start - lead, (3 * ks[c]) | (c << 16),
+                                   tp + ch * Qs[c]))
+                    continue
                 for s_, (qa, qb) in enumerate(((0, 3 * ks[c]), (3 * ks[c], Qs[c]))):
                     for q in range(qa, qb, 32):
                         vitems.append((v_off[c], Qs[c], q, min(32, qb - q), g0, g1, b.col.start - lead,
@@ -425,7 +439,7 @@ def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chu
     n = struct.n
     A.update(ditems=_rec(ditems, _lib.DENSE_ITEM), vitems=_rec(vitems, _lib.V_ITEM),
              utasks=_rec(utasks, _lib.U_TASK_M), n_ditems=len(ditems), n_vitems=len(vitems), n_utasks=len(utasks),
-             n_slots=slot, n_tpart=tp, n_scales=sb, kmax=kmax, u_sizes=u_off, v_sizes=v_off, pack=pack,
+             n_slots=slot, n_tpart=tp, n_scales=sb, kmax=kmax, u_sizes=u_off, v_sizes=v_off, pack=pack, stream=stream,
              class_terms=counts, alg_bytes=dense_entries * 6 * 4 + lr_bytes + 2 * n * 4 + 3 * n * 8)
     return A
 
@@ -490,6 +504,7 @@ class DeviceHMatrix:
         compiled library (the values its H-matrix assembly uses).  mixed_tol: the
         term-class tolerance of the "mixed" storage (classify_terms)."""
         self.mixed_tol = float(mixed_tol)
+        self.mixed_stream = True       # mixed storage: bulk-copy (streamed) low-rank kernels
         self.use_plan_cache = True
         import torch
         self.torch = torch
@@ -829,6 +844,11 @@ class DeviceHMatrix:
 
     def _mixed_arrays(self, cls_lists):
         dc, vc, ur = self.shapes("mixed")
+        if self.mixed_stream:
+            try:
+                return build_plan_arrays_mixed(self.s, self.dense_recs, cls_lists, dc, vc, ur, stream=True)
+            except _lib.Pq3dError:
+                pass                   # a term class too large for a stream stage: the plain kernels
         return build_plan_arrays_mixed(self.s, self.dense_recs, cls_lists, dc, vc, ur)
 
     def install_mixed(self, tmap, U, V, scales):
@@ -882,6 +902,10 @@ class DeviceHMatrix:
             hp["U16"], hp["U8"] = M["U"][1].data_ptr(), M["U"][2].data_ptr()
             hp["V16"], hp["V8"] = M["V"][1].data_ptr(), M["V"][2].data_ptr()
             hp["scales"] = M["scales"].data_ptr()
+            P["status"] = torch.zeros(1, dtype=torch.int32, device=self.dev)
+            hp["status"] = P["status"].data_ptr()
+            hp["stream"] = 1 if A.get("stream") else 0
+            P["stream"] = bool(A.get("stream"))
         P["host_plan"] = hp
         P["alg_bytes"] = A["alg_bytes"]
         P["stored_bytes"] = (P["dense"].numel() * P["dense"].element_size() if P["dense"] is not None else 0) + \
@@ -901,6 +925,12 @@ class DeviceHMatrix:
                 co += len(b.col.indices)
             self._ro_cache = res
         return self._ro_cache
+
+    def kernel_status(self, dtype):
+        """Status word of a plan's streamed kernels: 0, 1 after a timed-out wait, 2 after a
+        task of a size they do not take (nothing of the kind is expected)."""
+        P = self.plans.get(dtype)
+        return int(P["status"].item()) if P is not None and "status" in P else 0
 
     def new_x(self, dtype):
         """Zero deficit buffer (tree order, device layout of pack_x) for the given plan."""

@@ -78,7 +78,7 @@ def _weights(st, op, R):
     return out
 
 
-def pack_mixed(st, op, tol):
+def pack_mixed(st, op, tol, stream=False):
     recs, _, off32 = dense_layout([b for b in st.blocks if not b.aca])
     D = np.zeros(max(off32, 1), np.float32)
     for k, (b, ob) in enumerate(zip([b for b in st.blocks if not b.aca], [b for b in op.blocks if b[0] == "dense"])):
@@ -93,7 +93,7 @@ def pack_mixed(st, op, tol):
     R = _near_rowabs(st, op)
     W = _weights(st, op, R)
     cls_lists = [classify_terms(wS, wD, tol) for wS, wD in W]
-    A = build_plan_arrays_mixed(st, recs, cls_lists, dense_chunk=2, v_chunk=3, u_rows=40)
+    A = build_plan_arrays_mixed(st, recs, cls_lists, dense_chunk=2, v_chunk=3, u_rows=40, stream=stream)
     dt, fill = (np.float32, np.float16, np.uint8), (0, 0, 128)      # INT8 entries stored as b + 128
     U = [np.full(max(A["u_sizes"][c], 16), fill[c], dt[c]) for c in range(3)]
     V = [np.full(max(A["v_sizes"][c], 16), fill[c], dt[c]) for c in range(3)]
@@ -162,11 +162,18 @@ def emulate(st, A, D, U, V, scales, x):
                             x[2 * (int(it["c0"]) + g * 4 + t) + s]
         slots[3 * (int(it["slot"]) + rr)[:, None] + np.arange(3)] = acc
     for it in A["vitems"][:A["n_vitems"]]:
-        cls, slip = int(it["s"]) >> 8, int(it["s"]) & 255
+        if A.get("stream"):
+            # k_v_stream: all Q rows of one class; rows below 3 kS use the strike plane
+            cls, kS3 = int(it["s"]) >> 16, int(it["s"]) & 0xffff
+            assert int(it["q"]) == 0 and int(it["nr"]) == int(it["Q"])
+            assert int(it["Q"]) * 16 <= 12288 and (int(it["g1"]) - int(it["g0"])) * MIXED_CW[cls] <= 1024
+        else:
+            cls, kS3 = int(it["s"]) >> 8, None
         cw = MIXED_CW[cls]
         assert int(it["c0"]) % cw == 0
         Q, q0, nr = int(it["Q"]), int(it["q"]), int(it["nr"])
         for q in range(q0, q0 + nr):
+            slip = (0 if q < kS3 else 1) if kS3 is not None else int(it["s"]) & 255
             acc = 0.0
             for g in range(int(it["g0"]), int(it["g1"])):
                 idx = it["off"] + (g * Q + q) * cw + np.arange(cw)
@@ -209,10 +216,13 @@ def _reference(op, x1, x2):
                      op.mvm(x1, "Bs") + op.mvm(x2, "Bd")], axis=1)
 
 
+@pytest.mark.parametrize("stream", [False, True])
 @pytest.mark.parametrize("tol", [0.0, 2.0 ** -22, 2.0 ** -16])
-def test_mixed_matvec_emulation_within_bound(setup, tol):
+def test_mixed_matvec_emulation_within_bound(setup, tol, stream):
     st, op = setup
-    A, D, U, V, scales, R, cls = pack_mixed(st, op, tol)
+    A, D, U, V, scales, R, cls = pack_mixed(st, op, tol, stream)
+    if stream:
+        assert all(int(T["r1"]) - int(T["r0"]) <= 256 for T in A["utasks"][:A["n_utasks"]])
     rng = np.random.default_rng(7)
     x1, x2 = rng.standard_normal((2, st.n))
     x = pack_x(x1[st.perm], x2[st.perm], st.n)
