@@ -30,9 +30,17 @@ HM_PLAN = np.dtype([("n", "i4"), ("dtype", "i4")] + [(p, "u8") for p in _PLAN_PT
                    [(k, "i8") for k in ("n_ditems", "n_vitems", "n_utasks", "n_slots", "n_tpart")] +
                    [("kmax", "i4"), ("pad", "i4")] +
                    [(p, "u8") for p in ("U16", "V16", "U8", "V8", "scales", "status")] +
-                   [("stream", "i4"), ("pad2", "i4")], align=True)
-# streamed mixed kernels (hmatvec.cu): stage size, x-slice width and rows per U task
-STREAM_STAGE_BYTES, STREAM_XMAX, STREAM_ROWS = 12288, 1024, 256
+                   [("stream", "i4"), ("pad2", "i4")] +
+                   [(p, "u8") for p in ("tasks_a", "tasks_b", "cta_a", "cta_b", "gather", "tfull")] +
+                   [("n_gather", "i8"), ("ncta_a", "i4"), ("ncta_b", "i4")], align=True)
+# streamed mixed kernels (k_stream in hmatvec.cu): stage bytes, shared x/t buffer (floats),
+# the row limits of dense and U tasks
+STREAM_STAGE_BYTES, STREAM_BUF, STREAM_DENSE_ROWS, STREAM_ROWS = 12288, 3072, 128, 256
+STREAM_TASK = np.dtype([("off", "i8"), ("off1", "i8"), ("off2", "i8")] +
+                       [(k, "i4") for k in ("kind", "cls", "m", "r0", "r1", "g0", "g1", "c0", "out", "kS3",
+                                            "K0", "K1", "K2", "tb")], align=True)
+T_GATHER = np.dtype([(k, "i4", 3) for k in ("K", "kS", "kD", "Q", "tp", "nch", "sb")] + [("tb", "i4"), ("pad", "i4")],
+                    align=True)
 # mixed storage (FP32 / FP16 / INT8 term classes): U task and packing records
 U_TASK_M = np.dtype([("off", "i8", 3), ("m", "i4"), ("r0", "i4"), ("r1", "i4"), ("slot", "i4")] +
                     [(k, "i4", 3) for k in ("K", "kS", "kD", "Q", "tp", "nch", "sb")] + [("pad", "i4")], align=True)
@@ -109,6 +117,7 @@ def load():
     L.pq3d_item_bytes.restype = ctypes.c_size_t
     L.pq3d_hmatvec.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.pq3d_pack_mixed_task_bytes.restype = ctypes.c_size_t
+    L.pq3d_stream_ctas.restype = ctypes.c_int
     L.pq3d_nearfield_rowabs.argtypes = [vp, vp, i64, i32, vp, vp]
     L.pq3d_aca_term_weights.argtypes = [vp, i64, vp, vp, vp, vp, vp, vp]
     L.pq3d_aca_pack_mixed.argtypes = [vp, i64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
@@ -138,6 +147,7 @@ def load():
     sizes = {"DenseItem": (L.pq3d_item_bytes(0), DENSE_ITEM.itemsize), "VItem": (L.pq3d_item_bytes(1), V_ITEM.itemsize),
              "UTask": (L.pq3d_item_bytes(2), U_TASK.itemsize), "UTaskM": (L.pq3d_item_bytes(6), U_TASK_M.itemsize),
              "PackTaskM": (L.pq3d_pack_mixed_task_bytes(), PACK_TASK_M.itemsize),
+             "StreamTask": (L.pq3d_item_bytes(7), STREAM_TASK.itemsize), "TGather": (L.pq3d_item_bytes(8), T_GATHER.itemsize),
              "DenseBlock": (L.pq3d_item_bytes(4), DENSE_BLOCK.itemsize), "HmPlan": (L.pq3d_item_bytes(5), HM_PLAN.itemsize),
              "AcaTask": (L.pq3d_aca_task_bytes(), ACA_TASK.itemsize), "PackTask": (L.pq3d_pack_task_bytes(), PACK_TASK.itemsize),
              "RkArgs": (L.pq3d_rk_args_bytes(), RK_ARGS.itemsize),

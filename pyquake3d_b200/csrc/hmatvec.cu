@@ -513,29 +513,53 @@ k_du_mixed(const DenseItem *__restrict__ ditems, int64_t n_ditems, int64_t n_dbl
 }
 
 // ------------------------------------------------------------------ mixed storage, streamed
-// The same products as k_v_mixed / k_du_mixed, with the low-rank factors moved by
-// bulk copies: every task reads contiguous runs of the packed operator, so one
-// producer warp streams them into a ring of ST_STAGES shared-memory stages with
-// 1-D cp.async.bulk (global -> shared, completion counted in bytes on the stage's
-// "full" mbarrier) while eight consumer warps compute from shared memory and
-// release the stage on its "empty" mbarrier.  The loads no longer wait in
-// registers: a CTA keeps up to ST_STAGES * ST_STAGE_BYTES in flight.
-//   V task (VItem with q = 0, nr = Q, s = 3 kS | cls << 16): all Q rows of one
-//     class of one block over column groups [g0, g1) -- one contiguous range of
-//     (g1 - g0) Q 16-byte units; its x slices (strike and dip planes) sit in
-//     shared memory.  Threads map to (row, group residue) pairs; each group's
-//     partials are reduced across the residues at the end.
-//   U task (UTaskM, r1 - r0 <= ST_CONSUMERS): per class and column group, the
-//     three components' runs of rows [r0, r1) (three copies into one stage);
-//     one consumer thread per row.
-// All waits are bounded (ST_SPIN polls); a timeout stores 1 in *status, and the
-// producer still waits, bounded, for the copies it issued before the CTA exits.
+// The products of k_v_mixed / k_du_mixed with every byte of the packed operator
+// moved by bulk copies.  Each task reads contiguous runs, so in every CTA one
+// producer thread streams them with 1-D cp.async.bulk (global -> shared,
+// completion counted in bytes on the stage's "full" mbarrier) into a ring of
+// ST_STAGES stages, while eight consumer warps compute from shared memory and
+// release each stage on its "empty" mbarrier.  The CTAs are persistent: each
+// works through its own task list (balanced by bytes on the host), and the ring
+// runs on across task boundaries, so a small task costs no pipeline start-up.
+// The first piece of every task is what its consumers need besides the operator
+// (the x slices of its columns, or the block's t), so no task waits on a load.
+//   phase A, k_stream (kind 0 dense, kind 1 V):
+//     dense task: rows [r0, r1) (<= 128) of a dense block, column groups [g0, g1);
+//       x piece: the interleaved (strike, dip) deficit of its columns; data
+//       pieces: whole column groups, [group][6 operators][rows][16 B].
+//     V task: all Q rows of one term class of one low-rank block over column
+//       groups [g0, g1); x piece: the strike and dip planes of its columns; data
+//       pieces: whole groups, [group][Q][16 B].
+//   k_t_gather: per low-rank block, t of every class (sum of the V partials over
+//     the column chunks, times the FP16 / INT8 scales) into one contiguous run.
+//   phase B, k_stream (kind 2 U): rows [r0, r1) (<= 256) of a low-rank block; t
+//     piece, then per class and column group the three components' row runs.
+// Consumers map threads to (row, group residue) pairs and reduce the residues at
+// the end of a task, so short row sets keep every thread busy.  All waits are
+// bounded (ST_SPIN polls); a timeout stores 1 in *status, a task of a size the
+// plan builder never produces stores 2 and is skipped by producer and consumers
+// alike, and the producer waits (bounded) for the copies it issued before exit.
 constexpr int ST_STAGES = 4;
 constexpr int ST_STAGE_BYTES = 12288;
 constexpr int ST_CONSUMERS = 256;
 constexpr int ST_THREADS = ST_CONSUMERS + 32;
-constexpr int ST_XMAX = 1024;             // columns of a V task's x slices
+constexpr int ST_BUF = 3072;              // floats of a task's x slices or t in shared memory
 constexpr long long ST_SPIN = 1ll << 22;
+
+struct StreamTask {
+    int64_t off, off1, off2;   // dense: float offset of the block in D; V: element offset of the block in the
+                               // class's V array; U: element offsets in the FP32 / FP16 / INT8 U arrays
+    int32_t kind, cls;         // 0 dense, 1 V, 2 U; V: term class
+    int32_t m, r0, r1;         // dense / U: block rows and the task's row range; V: Q rows of the class
+    int32_t g0, g1, c0;        // dense / V: column groups, the block's aligned first column
+    int32_t out;               // dense / U: slot of block row 0; V: tpart offset of this chunk
+    int32_t kS3;               // V: rows below kS3 use the strike plane
+    int32_t K0, K1, K2, tb;    // U: class column counts, offset of the block's t in tfull
+};
+
+struct TGather {               // one low-rank block: its classes' V rows, partials, scales, t offset
+    int32_t K[3], kS[3], kD[3], Q[3], tp[3], nch[3], sb[3], tb, pad;
+};
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -545,16 +569,13 @@ __device__ __forceinline__ void mbar_init(uint64_t *b, unsigned count)
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *b, unsigned bytes)
 {
-    uint64_t st;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
-                 : "=l"(st) : "r"(smem_addr(b)), "r"(bytes) : "memory");
-    (void)st;
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}"
+                 ::"r"(smem_addr(b)), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t *b)
 {
-    uint64_t st;
-    asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];" : "=l"(st) : "r"(smem_addr(b)) : "memory");
-    (void)st;
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}"
+                 ::"r"(smem_addr(b)) : "memory");
 }
 // Bounded wait for the phase of parity `parity` to complete; false on timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity)
@@ -571,7 +592,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity)
     return false;
 }
 // 1-D bulk copy global -> this CTA's shared memory; completion counted on `bar`.
-// dst, src 16-byte aligned, bytes a multiple of 16.
+// dst, src 16-byte aligned, bytes a multiple of 16 (the layouts guarantee both).
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar)
 {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
@@ -579,26 +600,7 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
 }
 __device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, %0;" ::"n"(ST_CONSUMERS) : "memory"); }
 
-__device__ __forceinline__ void st_init_barriers(uint64_t *full, uint64_t *empty)
-{
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < ST_STAGES; ++s) {
-            mbar_init(full + s, 1);                     // the producer's arrive.expect_tx
-            mbar_init(empty + s, ST_CONSUMERS / 32);    // one arrive per consumer warp
-        }
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-}
-
-// Producer epilogue: bounded wait for the copies of the last pieces it issued.
-__device__ __forceinline__ void st_drain(uint64_t *full, int issued, int *status)
-{
-    for (int i = issued > ST_STAGES ? issued - ST_STAGES : 0; i < issued; ++i)
-        if (!mbar_wait(full + i % ST_STAGES, (unsigned)(i / ST_STAGES) & 1u)) atomicExch(status, 1);
-}
-
-// dot of one 16-byte unit of class element type TL with CW floats of x (or t)
+// dot of one 16-byte unit of class element type TL with CW floats
 template <typename TL>
 __device__ __forceinline__ float dot16(const unsigned char *u, const float *xv)
 {
@@ -622,170 +624,321 @@ __device__ __forceinline__ float dot16(const unsigned char *u, const float *xv)
     return a;
 }
 
+__device__ __forceinline__ int cw_of(int cls) { return cls == 0 ? 4 : (cls == 1 ? 8 : 16); }
+
+// Sizes the plan builder produces; anything else is skipped (status 2).
+__device__ __forceinline__ bool task_ok(const StreamTask &T)
+{
+    const int G = T.g1 - T.g0;
+    if (T.kind == 0) {
+        const int R = T.r1 - T.r0;
+        return R >= 1 && R <= 128 && T.r0 >= 0 && T.r1 <= T.m && G >= 1 && 8 * G <= ST_BUF;
+    }
+    if (T.kind == 1)
+        return T.cls >= 0 && T.cls <= 2 && T.m >= 1 && T.m * 16 <= ST_STAGE_BYTES && G >= 1 &&
+               2 * G * cw_of(T.cls) <= ST_BUF && T.kS3 >= 0 && T.kS3 <= T.m;
+    if (T.kind == 2) {
+        const int R = T.r1 - T.r0;
+        return R >= 1 && R <= ST_CONSUMERS && T.r0 >= 0 && T.r1 <= T.m && T.K0 >= 0 && T.K1 >= 0 && T.K2 >= 0 &&
+               T.K0 % 4 == 0 && T.K1 % 8 == 0 && T.K2 % 16 == 0 && 3 * (T.K0 + T.K1 + T.K2) <= ST_BUF;
+    }
+    return false;
+}
+
+// Groups per data piece of dense (R rows) and V (Q rows) tasks.
+__device__ __forceinline__ int dense_gp(int R) { return ST_STAGE_BYTES / (6 * R * 16); }
+__device__ __forceinline__ int v_gp(int Q) { return ST_STAGE_BYTES / (Q * 16); }
+
+__device__ __forceinline__ int task_pieces(const StreamTask &T)
+{
+    const int G = T.g1 - T.g0;
+    if (T.kind == 0) { const int gp = dense_gp(T.r1 - T.r0); return 1 + (G + gp - 1) / gp; }
+    if (T.kind == 1) { const int gp = v_gp(T.m); return 1 + (G + gp - 1) / gp; }
+    return 1 + T.K0 / 4 + T.K1 / 8 + T.K2 / 16;
+}
+
+struct StreamArgs {
+    const StreamTask *tasks;
+    const int32_t *cta_ptr;    // tasks [cta_ptr[b], cta_ptr[b + 1]) belong to CTA b
+    const float *D;            // FP32 dense blocks
+    const void *V[3], *U[3];   // class arrays (FP32, FP16, INT8)
+    const float *x;            // deficit (hm_layout.cuh)
+    int xstride;
+    float *tpart, *slots;
+    const float *tfull;
+    int *status;
+};
+
+// Producer: issue the copies of piece `p` of task T into stage s.
+__device__ __forceinline__ void issue_piece(const StreamArgs &A, const StreamTask &T, int p, unsigned char *dst,
+                                            uint64_t *bar)
+{
+    const int G = T.g1 - T.g0;
+    if (T.kind == 0) {
+        const int R = T.r1 - T.r0;
+        if (p == 0) {
+            const unsigned nb = (unsigned)(32 * G);
+            mbar_expect_tx(bar, nb);
+            bulk_g2s(dst, A.x + 2 * ((int64_t)T.c0 + (int64_t)T.g0 * 4), nb, bar);
+            return;
+        }
+        const int gp = dense_gp(R), ga = (p - 1) * gp, gb = min(G, ga + gp);
+        if (R == T.m) {                                   // whole rows: the piece is one run
+            const unsigned nb = (unsigned)((gb - ga) * 6 * R * 16);
+            mbar_expect_tx(bar, nb);
+            bulk_g2s(dst, A.D + T.off + ((int64_t)(T.g0 + ga) * 6 * T.m) * 4, nb, bar);
+        } else {
+            mbar_expect_tx(bar, (unsigned)((gb - ga) * 6 * R * 16));
+            for (int g = ga; g < gb; ++g)
+                for (int op = 0; op < 6; ++op)
+                    bulk_g2s(dst + ((size_t)(g - ga) * 6 + op) * R * 16,
+                             A.D + T.off + (((int64_t)(T.g0 + g) * 6 + op) * T.m + T.r0) * 4, (unsigned)(R * 16), bar);
+        }
+        return;
+    }
+    if (T.kind == 1) {
+        const int CW = cw_of(T.cls), Q = T.m;
+        if (p == 0) {
+            const unsigned nb = (unsigned)(G * CW * 4);
+            mbar_expect_tx(bar, 2 * nb);
+            const float *xs = A.x + T.c0 + (int64_t)T.g0 * CW;
+            bulk_g2s(dst, xs + 2 * (int64_t)A.xstride, nb, bar);
+            bulk_g2s(dst + nb, xs + 3 * (int64_t)A.xstride, nb, bar);
+            return;
+        }
+        const int gp = v_gp(Q), ga = (p - 1) * gp, gb = min(G, ga + gp);
+        const unsigned nb = (unsigned)((gb - ga) * Q * 16);
+        mbar_expect_tx(bar, nb);
+        const void *Vc = T.cls == 0 ? A.V[0] : (T.cls == 1 ? A.V[1] : A.V[2]);
+        bulk_g2s(dst, reinterpret_cast<const unsigned char *>(Vc) + (T.off + (int64_t)(T.g0 + ga) * Q * CW) * (16 / CW),
+                 nb, bar);
+        return;
+    }
+    const int R = T.r1 - T.r0;
+    if (p == 0) {
+        const unsigned nb = (unsigned)(3 * (T.K0 + T.K1 + T.K2) * 4);
+        mbar_expect_tx(bar, nb);
+        bulk_g2s(dst, A.tfull + T.tb, nb, bar);
+        return;
+    }
+    int q = p - 1, cls = 0;
+    const int n0 = T.K0 / 4, n1 = T.K1 / 8;
+    if (q >= n0) { q -= n0; cls = 1; if (q >= n1) { q -= n1; cls = 2; } }
+    const int64_t off = cls == 0 ? T.off : (cls == 1 ? T.off1 : T.off2);
+    const void *Uc = cls == 0 ? A.U[0] : (cls == 1 ? A.U[1] : A.U[2]);
+    const unsigned char *base = reinterpret_cast<const unsigned char *>(Uc) + off * (cls == 0 ? 4 : (cls == 1 ? 2 : 1));
+    mbar_expect_tx(bar, (unsigned)(3 * R * 16));
+    for (int c = 0; c < 3; ++c)
+        bulk_g2s(dst + (size_t)c * R * 16, base + (((int64_t)q * 3 + c) * T.m + T.r0) * 16, (unsigned)(R * 16), bar);
+}
+
 template <typename TL>
-__device__ void v_task_stream(const VItem &T, const TL *__restrict__ Vc, const float *__restrict__ x, int xstride,
-                              float *__restrict__ tpart, unsigned char *stage, uint64_t *full, uint64_t *empty,
-                              float *xs, float *red, int *status)
+__device__ __forceinline__ void consume_v_piece(const unsigned char *st, const float *xs, int Q, int kS3, int ga,
+                                                int gb, int ga0, int q0, int res, int R, float &acc)
 {
     constexpr int CW = 16 / sizeof(TL);
-    const int Q = T.Q, G = T.g1 - T.g0, kS3 = T.s & 0xffff;
-    // sizes the plan builder never produces: reject before any barrier or copy
-    if (Q <= 0 || Q * 16 > ST_STAGE_BYTES || G <= 0 || G * CW > ST_XMAX) {
-        if (threadIdx.x == 0) atomicExch(status, 2);
-        return;
-    }
-    const int gp = ST_STAGE_BYTES / (Q * 16);                        // whole groups per piece (>= 1)
-    const int npieces = (G + gp - 1) / gp;
-    const unsigned char *src = reinterpret_cast<const unsigned char *>(Vc + T.off) + (int64_t)T.g0 * Q * 16;
+    for (int g = ga + ((res - ga) % R + R) % R; g < gb; g += R)     // the piece's groups of residue res
+        acc += dot16<TL>(st + ((size_t)(g - ga0) * Q + q0) * 16, xs + (q0 < kS3 ? 0 : ST_BUF / 2) + g * CW);
+}
+
+__global__ void __launch_bounds__(ST_THREADS, 1) k_stream(StreamArgs A)
+{
+    extern __shared__ __align__(128) unsigned char sm[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(sm), *empty = full + ST_STAGES;
+    float *buf = reinterpret_cast<float *>(sm + 128);                    // x slices or t
+    float *red = buf + ST_BUF;                                           // 3 x ST_CONSUMERS
+    unsigned char *stage = reinterpret_cast<unsigned char *>(red + 3 * ST_CONSUMERS);
     const int tid = threadIdx.x;
-    if (tid >= ST_CONSUMERS) {                                       // producer warp
-        if (tid == ST_CONSUMERS) {
-            int i = 0;
-            for (; i < npieces; ++i) {
+    if (tid == 0) {
+        for (int s = 0; s < ST_STAGES; ++s) {
+            mbar_init(full + s, 1);                         // the producer's arrive.expect_tx
+            mbar_init(empty + s, ST_CONSUMERS / 32);        // one arrive per consumer warp
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const int t0 = A.cta_ptr[blockIdx.x], t1 = A.cta_ptr[blockIdx.x + 1];
+    if (tid >= ST_CONSUMERS) {
+        // ---------------------------------------------------------- producer
+        if (tid != ST_CONSUMERS) return;
+        int i = 0;
+        bool stop = false;
+        for (int t = t0; t < t1 && !stop; ++t) {
+            const StreamTask T = A.tasks[t];
+            if (!task_ok(T)) { atomicExch(A.status, 2); continue; }
+            const int np = task_pieces(T);
+            for (int p = 0; p < np; ++p, ++i) {
                 const int s = i % ST_STAGES;
                 if (i >= ST_STAGES && !mbar_wait(empty + s, (unsigned)(i / ST_STAGES - 1) & 1u)) {
-                    atomicExch(status, 1);
+                    atomicExch(A.status, 1);
+                    stop = true;
                     break;
                 }
-                const int ga = i * gp, ng = min(gp, G - ga);
-                const unsigned nb = (unsigned)(ng * Q * 16);
-                mbar_expect_tx(full + s, nb);
-                bulk_g2s(stage + (size_t)s * ST_STAGE_BYTES, src + (int64_t)ga * Q * 16, nb, full + s);
+                issue_piece(A, T, p, stage + (size_t)s * ST_STAGE_BYTES, full + s);
             }
-            st_drain(full, i, status);
         }
+        for (int k = i > ST_STAGES ? i - ST_STAGES : 0; k < i; ++k)      // the copies still in flight
+            if (!mbar_wait(full + k % ST_STAGES, (unsigned)(k / ST_STAGES) & 1u)) atomicExch(A.status, 1);
         return;
     }
-    // x slices of the task's columns (strike and dip planes)
-    const float *xg = x + T.c0 + (int64_t)T.g0 * CW;
-    for (int c = tid; c < G * CW; c += ST_CONSUMERS) {
-        xs[c] = xg[2 * (int64_t)xstride + c];
-        xs[ST_XMAX + c] = xg[3 * (int64_t)xstride + c];
-    }
-    consumers_sync();
-    // thread -> (row q, group residue r): R residues when Q <= 256, else rows tid, tid + 256, ...
-    const int R = Q <= ST_CONSUMERS ? ST_CONSUMERS / Q : 1;
-    const bool act = tid < R * Q || Q > ST_CONSUMERS;
-    const int q0 = Q <= ST_CONSUMERS ? tid % Q : tid, r = Q <= ST_CONSUMERS ? tid / Q : 0;
-    float acc[3] = {0.f, 0.f, 0.f};
-    for (int i = 0; i < npieces; ++i) {
-        const int s = i % ST_STAGES;
-        const bool ok = mbar_wait(full + s, (unsigned)(i / ST_STAGES) & 1u);
-        if (!ok) atomicExch(status, 1);
-        if (ok && act) {
-            const unsigned char *st = stage + (size_t)s * ST_STAGE_BYTES;
-            const int ga = i * gp, gb = min(G, ga + gp);
-            for (int g = ga + r; g < gb; g += R) {
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const int q = q0 + k * ST_CONSUMERS;
-                    if (q < Q && (k == 0 || Q > ST_CONSUMERS))
-                        acc[k] += dot16<TL>(st + ((size_t)(g - ga) * Q + q) * 16, xs + (q < kS3 ? 0 : ST_XMAX) + g * CW);
+    // -------------------------------------------------------------- consumers
+    int i = 0;
+    for (int t = t0; t < t1; ++t) {
+        const StreamTask T = A.tasks[t];
+        if (!task_ok(T)) continue;
+        const int np = task_pieces(T), G = T.g1 - T.g0;
+        // piece 0: x slices / t into buf
+        {
+            const int s = i % ST_STAGES;
+            const bool ok = mbar_wait(full + s, (unsigned)(i / ST_STAGES) & 1u);
+            if (!ok) atomicExch(A.status, 1);
+            const float *st = reinterpret_cast<const float *>(stage + (size_t)s * ST_STAGE_BYTES);
+            if (T.kind == 0) {
+                for (int e = tid; e < 8 * G; e += ST_CONSUMERS) buf[e] = ok ? st[e] : 0.f;
+            } else if (T.kind == 1) {
+                const int w = G * cw_of(T.cls);
+                for (int e = tid; e < w; e += ST_CONSUMERS) {
+                    buf[e] = ok ? st[e] : 0.f;
+                    buf[ST_BUF / 2 + e] = ok ? st[w + e] : 0.f;
                 }
+            } else {
+                for (int e = tid; e < 3 * (T.K0 + T.K1 + T.K2); e += ST_CONSUMERS) buf[e] = ok ? st[e] : 0.f;
             }
+            __syncwarp();
+            if ((tid & 31) == 0) mbar_arrive(empty + s);
+            ++i;
+            consumers_sync();
         }
-        __syncwarp();
-        if ((tid & 31) == 0) mbar_arrive(empty + s);
-    }
-    if (Q <= ST_CONSUMERS) {
-        red[tid] = act ? acc[0] : 0.f;
-        consumers_sync();
-        if (tid < Q) {
-            float v = 0.f;
-            for (int rr = 0; rr < R; ++rr) v += red[rr * Q + tid];
-            tpart[T.tp + tid] = v;
-        }
-    } else {
+        if (T.kind == 0) {
+            // ---- dense: thread -> (row, group residue)
+            const int R = T.r1 - T.r0, RR = ST_CONSUMERS / R, gp = dense_gp(R);
+            const int tr = tid % R, res = tid / R;
+            const bool act = res < RR;
+            float acc[3] = {0.f, 0.f, 0.f};
+            for (int p = 1; p < np; ++p, ++i) {
+                const int s = i % ST_STAGES;
+                const bool ok = mbar_wait(full + s, (unsigned)(i / ST_STAGES) & 1u);
+                if (!ok) atomicExch(A.status, 1);
+                const int ga = (p - 1) * gp, gb = min(G, ga + gp);
+                if (ok && act) {
+                    const unsigned char *st = stage + (size_t)s * ST_STAGE_BYTES;
+                    for (int g = ga + ((res - ga) % RR + RR) % RR; g < gb; g += RR) {
+                        const float *xv = buf + 8 * g;
 #pragma unroll
-        for (int k = 0; k < 3; ++k)
-            if (q0 + k * ST_CONSUMERS < Q) tpart[T.tp + q0 + k * ST_CONSUMERS] = acc[k];
-    }
-}
-
-__global__ void __launch_bounds__(ST_THREADS, 1)
-k_v_stream(const VItem *__restrict__ tasks, const float *__restrict__ V32, const __half *__restrict__ V16,
-           const uint8_t *__restrict__ V8, const float *__restrict__ x, int xstride, float *__restrict__ tpart,
-           int *status)
-{
-    asm volatile("griddepcontrol.launch_dependents;");
-    extern __shared__ __align__(128) unsigned char sm[];
-    uint64_t *full = reinterpret_cast<uint64_t *>(sm), *empty = full + ST_STAGES;
-    float *xs = reinterpret_cast<float *>(sm + 128);
-    float *red = xs + 2 * ST_XMAX;
-    unsigned char *stage = sm + 128 + (2 * ST_XMAX + ST_CONSUMERS) * 4;
-    st_init_barriers(full, empty);
-    const VItem T = tasks[blockIdx.x];
-    const int cls = T.s >> 16;
-    if (cls == 0) v_task_stream<float>(T, V32, x, xstride, tpart, stage, full, empty, xs, red, status);
-    else if (cls == 1) v_task_stream<__half>(T, V16, x, xstride, tpart, stage, full, empty, xs, red, status);
-    else v_task_stream<uint8_t>(T, V8, x, xstride, tpart, stage, full, empty, xs, red, status);
-}
-
-// Dense items (nine warps per CTA), then U tasks with bulk-copied factors.  The
-// producer starts streaming U right away (it does not depend on k_v_stream); the
-// consumers wait for k_v_stream (griddepcontrol.wait) before gathering t.
-__global__ void __launch_bounds__(ST_THREADS, 1)
-k_du_stream(const DenseItem *__restrict__ ditems, int64_t n_ditems, int64_t n_dblocks,
-            const UTaskM *__restrict__ tasks, const float *__restrict__ D, const float *__restrict__ U32,
-            const __half *__restrict__ U16, const uint8_t *__restrict__ U8, const float *__restrict__ x,
-            float *__restrict__ slots, const float *__restrict__ tpart, const float *__restrict__ scales,
-            int *status)
-{
-    if (blockIdx.x < n_dblocks) {
-        const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-        dense_v_item<float, float, float>(w, ditems, n_ditems, nullptr, 0, D, nullptr, x, 0, slots, nullptr);
-        return;
-    }
-    extern __shared__ __align__(128) unsigned char sm[];
-    uint64_t *full = reinterpret_cast<uint64_t *>(sm), *empty = full + ST_STAGES;
-    unsigned char *stage = sm + 128;
-    float *ts = reinterpret_cast<float *>(stage + (size_t)ST_STAGES * ST_STAGE_BYTES);
-    st_init_barriers(full, empty);
-    const UTaskM T = tasks[blockIdx.x - n_dblocks];
-    const int rows = T.r1 - T.r0;
-    if (rows <= 0 || rows > ST_CONSUMERS) {                          // the plan builder never produces these
-        if (threadIdx.x == 0) atomicExch(status, 2);
-        return;
-    }
-    const int ng0 = T.K[0] / 4, ng1 = T.K[1] / 8, ng2 = T.K[2] / 16;
-    const int tid = threadIdx.x;
-    const unsigned run = (unsigned)rows * 16u;                       // bytes of one component's rows
-    if (tid >= ST_CONSUMERS) {                                       // producer warp
-        if (tid == ST_CONSUMERS) {
-            int i = 0;
-            bool stop = false;
-#pragma unroll 1
-            for (int cls = 0; cls < 3 && !stop; ++cls) {
-                const unsigned char *base =
-                    cls == 0 ? reinterpret_cast<const unsigned char *>(U32 + T.off[0])
-                             : (cls == 1 ? reinterpret_cast<const unsigned char *>(U16 + T.off[1])
-                                         : reinterpret_cast<const unsigned char *>(U8 + T.off[2]));
-                const int ngc = cls == 0 ? ng0 : (cls == 1 ? ng1 : ng2);
-                for (int g = 0; g < ngc; ++g, ++i) {
-                    const int s = i % ST_STAGES;
-                    if (i >= ST_STAGES && !mbar_wait(empty + s, (unsigned)(i / ST_STAGES - 1) & 1u)) {
-                        atomicExch(status, 1);
-                        stop = true;
-                        break;
+                        for (int c = 0; c < 3; ++c)
+#pragma unroll
+                            for (int sl = 0; sl < 2; ++sl) {
+                                const float4 d = *reinterpret_cast<const float4 *>(
+                                    st + (((size_t)(g - ga) * 6 + 2 * c + sl) * R + tr) * 16);
+                                acc[c] += d.x * xv[sl] + d.y * xv[2 + sl] + d.z * xv[4 + sl] + d.w * xv[6 + sl];
+                            }
                     }
-                    mbar_expect_tx(full + s, 3 * run);
-                    unsigned char *dst = stage + (size_t)s * ST_STAGE_BYTES;
-                    for (int c = 0; c < 3; ++c)
-                        bulk_g2s(dst + c * run, base + (((int64_t)g * 3 + c) * T.m + T.r0) * 16, run, full + s);
+                }
+                __syncwarp();
+                if ((tid & 31) == 0) mbar_arrive(empty + s);
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) red[c * ST_CONSUMERS + tid] = act ? acc[c] : 0.f;
+            consumers_sync();
+            if (tid < R) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    float v = 0.f;
+                    for (int r = 0; r < RR; ++r) v += red[c * ST_CONSUMERS + r * R + tid];
+                    A.slots[3 * ((int64_t)T.out + T.r0 + tid) + c] = v;
                 }
             }
-            st_drain(full, i, status);
+        } else if (T.kind == 1) {
+            // ---- V: thread -> (row q, group residue); rows beyond 256 in a second pass
+            const int Q = T.m, gp = v_gp(Q);
+            const int RR = Q <= ST_CONSUMERS ? ST_CONSUMERS / Q : 1;
+            const int q0 = Q <= ST_CONSUMERS ? tid % Q : tid, res = Q <= ST_CONSUMERS ? tid / Q : 0;
+            const bool act = Q <= ST_CONSUMERS ? res < RR : true;
+            float acc[3] = {0.f, 0.f, 0.f};
+            for (int p = 1; p < np; ++p, ++i) {
+                const int s = i % ST_STAGES;
+                const bool ok = mbar_wait(full + s, (unsigned)(i / ST_STAGES) & 1u);
+                if (!ok) atomicExch(A.status, 1);
+                const int ga = (p - 1) * gp, gb = min(G, ga + gp);
+                if (ok && act) {
+                    const unsigned char *st = stage + (size_t)s * ST_STAGE_BYTES;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const int q = q0 + k * ST_CONSUMERS;
+                        if (q < Q && (k == 0 || Q > ST_CONSUMERS)) {
+                            if (T.cls == 0) consume_v_piece<float>(st, buf, Q, T.kS3, ga, gb, ga, q, res, RR, acc[k]);
+                            else if (T.cls == 1) consume_v_piece<__half>(st, buf, Q, T.kS3, ga, gb, ga, q, res, RR, acc[k]);
+                            else consume_v_piece<uint8_t>(st, buf, Q, T.kS3, ga, gb, ga, q, res, RR, acc[k]);
+                        }
+                    }
+                }
+                __syncwarp();
+                if ((tid & 31) == 0) mbar_arrive(empty + s);
+            }
+            if (Q <= ST_CONSUMERS) {
+                red[tid] = act ? acc[0] : 0.f;
+                consumers_sync();
+                if (tid < Q) {
+                    float v = 0.f;
+                    for (int r = 0; r < RR; ++r) v += red[r * Q + tid];
+                    A.tpart[T.out + tid] = v;
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    if (q0 + k * ST_CONSUMERS < Q) A.tpart[T.out + q0 + k * ST_CONSUMERS] = acc[k];
+            }
+        } else {
+            // ---- U: one thread per row
+            const int R = T.r1 - T.r0;
+            const bool act = tid < R;
+            float acc[3] = {0.f, 0.f, 0.f};
+            const int n0 = T.K0 / 4, n1 = T.K1 / 8;
+            for (int p = 1; p < np; ++p, ++i) {
+                const int s = i % ST_STAGES;
+                const bool ok = mbar_wait(full + s, (unsigned)(i / ST_STAGES) & 1u);
+                if (!ok) atomicExch(A.status, 1);
+                if (ok && act) {
+                    const unsigned char *st = stage + (size_t)s * ST_STAGE_BYTES + (size_t)tid * 16;
+                    const int q = p - 1;
+                    if (q < n0) {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) acc[c] += dot16<float>(st + (size_t)c * R * 16, buf + c * T.K0 + q * 4);
+                    } else if (q < n0 + n1) {
+                        const float *tc = buf + 3 * T.K0;
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+                            acc[c] += dot16<__half>(st + (size_t)c * R * 16, tc + c * T.K1 + (q - n0) * 8);
+                    } else {
+                        const float *tc = buf + 3 * (T.K0 + T.K1);
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+                            acc[c] += dot16<uint8_t>(st + (size_t)c * R * 16, tc + c * T.K2 + (q - n0 - n1) * 16);
+                    }
+                }
+                __syncwarp();
+                if ((tid & 31) == 0) mbar_arrive(empty + s);
+            }
+            if (act) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) A.slots[3 * ((int64_t)T.out + T.r0 + tid) + c] = acc[c];
+            }
         }
-        return;
+        consumers_sync();      // buf and red are reused by the next task
     }
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    // t of every class (scaled), as u_task_mixed
-    const int base1 = 3 * T.K[0], base2 = 3 * (T.K[0] + T.K[1]);
+}
+
+// t of every class of every low-rank block (as the U tasks of k_du_mixed gather it):
+// one CTA per block, t_c[c][q] = scale * sum over chunks of the V partials.
+__global__ void __launch_bounds__(128) k_t_gather(const TGather *__restrict__ gs, const float *__restrict__ tpart,
+                                                  const float *__restrict__ scales, float *__restrict__ tfull)
+{
+    const TGather T = gs[blockIdx.x];
+    float *o = tfull + T.tb;
 #pragma unroll
     for (int cls = 0; cls < 3; ++cls) {
         const int K = T.K[cls], kS = T.kS[cls], kD = T.kD[cls];
-        float *tc = ts + (cls == 0 ? 0 : (cls == 1 ? base1 : base2));
-        for (int e = tid; e < 3 * K; e += ST_CONSUMERS) {
+        for (int e = threadIdx.x; e < 3 * K; e += blockDim.x) {
             const int c = e / K, q = e % K;
             int row = -1;
             if (q < kS) row = c * kS + q;
@@ -795,38 +948,9 @@ k_du_stream(const DenseItem *__restrict__ ditems, int64_t n_ditems, int64_t n_db
                 v = sum_partials<float>(tpart + T.tp[cls] + row, T.nch[cls], T.Q[cls]);
                 if (cls > 0) v *= scales[T.sb[cls] + row];
             }
-            tc[e] = v;
+            o[e] = v;
         }
-    }
-    consumers_sync();
-    float acc[3] = {0.f, 0.f, 0.f};
-    const bool act = tid < rows;
-    int i = 0;
-#pragma unroll 1
-    for (int cls = 0; cls < 3; ++cls) {
-        const int K = cls == 0 ? T.K[0] : (cls == 1 ? T.K[1] : T.K[2]);
-        const int ngc = cls == 0 ? ng0 : (cls == 1 ? ng1 : ng2);
-        const float *tc = ts + (cls == 0 ? 0 : (cls == 1 ? base1 : base2));
-        for (int g = 0; g < ngc; ++g, ++i) {
-            const int s = i % ST_STAGES;
-            const bool ok = mbar_wait(full + s, (unsigned)(i / ST_STAGES) & 1u);
-            if (!ok) atomicExch(status, 1);
-            if (ok && act) {
-                const unsigned char *st = stage + (size_t)s * ST_STAGE_BYTES + (size_t)tid * 16;
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    if (cls == 0) acc[c] += dot16<float>(st + c * run, tc + c * K + g * 4);
-                    else if (cls == 1) acc[c] += dot16<__half>(st + c * run, tc + c * K + g * 8);
-                    else acc[c] += dot16<uint8_t>(st + c * run, tc + c * K + g * 16);
-                }
-            }
-            __syncwarp();
-            if ((tid & 31) == 0) mbar_arrive(empty + s);
-        }
-    }
-    if (act) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) slots[3 * ((int64_t)T.slot + T.r0 + tid) + c] = acc[c];
+        o += 3 * K;
     }
 }
 
@@ -893,8 +1017,14 @@ struct HmPlan {
     // storage code 3 only (U, V above are the FP32 class arrays)
     const void *U16, *V16, *U8, *V8;   // FP16 and INT8 class arrays
     const float *scales;               // per-V-row scales of the FP16 and INT8 classes
-    int32_t *status;                   // streamed kernels: 1 after a timed-out wait (else untouched)
-    int32_t stream, pad2;              // 1: the low-rank work runs in k_v_stream / k_du_stream
+    int32_t *status;                   // streamed kernels: 1 after a timed-out wait, 2 after a skipped task
+    int32_t stream, pad2;              // 1: the streamed kernels (k_stream, k_t_gather) run the plan
+    const void *tasks_a, *tasks_b;     // StreamTask lists: phase A (dense, V), phase B (U), grouped by CTA
+    const int32_t *cta_a, *cta_b;      // per-CTA ranges of the task lists (ncta + 1 entries)
+    const void *gather;                // TGather per low-rank block
+    float *tfull;                      // the blocks' t, written by k_t_gather
+    int64_t n_gather;
+    int32_t ncta_a, ncta_b;
 };
 
 PQ3D_EXPORT size_t pq3d_item_bytes(int kind)
@@ -906,6 +1036,8 @@ PQ3D_EXPORT size_t pq3d_item_bytes(int kind)
     case 4: return sizeof(DenseBlock);
     case 5: return sizeof(HmPlan);
     case 6: return sizeof(UTaskM);
+    case 7: return sizeof(StreamTask);
+    case 8: return sizeof(TGather);
     }
     return 0;
 }
@@ -1003,42 +1135,59 @@ static int run_matvec_mixed(const HmPlan &P, const float *x, float *slots, float
     return pq3d_launch_status();
 }
 
-// Storage code 3 with streamed low-rank work (plan.stream = 1).
+// Storage code 3, streamed: phase A (dense and V tasks), the t gather, phase B (U tasks).
+static size_t stream_smem() { return 128 + (size_t)(ST_BUF + 3 * ST_CONSUMERS) * 4 + (size_t)ST_STAGES * ST_STAGE_BYTES; }
+
 static int run_matvec_stream(const HmPlan &P, const float *x, float *slots, float *tpart, const double *add0,
                              const double *add1, const double *add2, double *y, cudaStream_t st)
 {
-    if (!P.status) return PQ3D_ERR_ARG;
-    const size_t smv = 128 + (2 * ST_XMAX + ST_CONSUMERS) * 4 + (size_t)ST_STAGES * ST_STAGE_BYTES;
-    const size_t smu = 128 + (size_t)ST_STAGES * ST_STAGE_BYTES + (size_t)3 * P.kmax * sizeof(float);
-    if (smu > 200 * 1024) return PQ3D_ERR_ARG;
-    PQ3D_CHECK(cudaFuncSetAttribute(k_v_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smv));
-    PQ3D_CHECK(cudaFuncSetAttribute(k_du_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smu));
-    if (P.n_vitems > 0)
-        k_v_stream<<<(unsigned)P.n_vitems, ST_THREADS, smv, st>>>((const VItem *)P.vitems, (const float *)P.V,
-                                                                  (const __half *)P.V16, (const uint8_t *)P.V8, x,
-                                                                  x_stride(P.n), tpart, P.status);
-    const int64_t n_dblocks = (P.n_ditems * 32 + ST_THREADS - 1) / ST_THREADS;
-    const int64_t grid = n_dblocks + P.n_utasks;
-    if (grid > 0) {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)grid);
-        cfg.blockDim = dim3(ST_THREADS);
-        cfg.dynamicSmemBytes = smu;
-        cfg.stream = st;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = P.n_vitems > 0 ? 1 : 0;
-        PQ3D_CHECK(cudaLaunchKernelEx(&cfg, k_du_stream, (const DenseItem *)P.ditems, P.n_ditems, n_dblocks,
-                                      (const UTaskM *)P.utasks, (const float *)P.dense, (const float *)P.U,
-                                      (const __half *)P.U16, (const uint8_t *)P.U8, x, slots, (const float *)tpart,
-                                      P.scales, P.status));
+    if (!P.status || (P.ncta_a > 0 && (!P.tasks_a || !P.cta_a)) || (P.ncta_b > 0 && (!P.tasks_b || !P.cta_b)) ||
+        (P.n_gather > 0 && (!P.gather || !P.tfull)))
+        return PQ3D_ERR_ARG;
+    const size_t sm = stream_smem();
+    PQ3D_CHECK(cudaFuncSetAttribute(k_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    StreamArgs A;
+    A.D = (const float *)P.dense;
+    A.V[0] = P.V; A.V[1] = P.V16; A.V[2] = P.V8;
+    A.U[0] = P.U; A.U[1] = P.U16; A.U[2] = P.U8;
+    A.x = x;
+    A.xstride = x_stride(P.n);
+    A.tpart = tpart;
+    A.slots = slots;
+    A.tfull = P.tfull;
+    A.status = P.status;
+    if (P.ncta_a > 0) {
+        A.tasks = (const StreamTask *)P.tasks_a;
+        A.cta_ptr = P.cta_a;
+        k_stream<<<(unsigned)P.ncta_a, ST_THREADS, sm, st>>>(A);
+    }
+    if (P.n_gather > 0) {
+        if (P.n_gather > 0x7fffffff) return PQ3D_ERR_ARG;
+        k_t_gather<<<(unsigned)P.n_gather, 128, 0, st>>>((const TGather *)P.gather, tpart, P.scales, P.tfull);
+    }
+    if (P.ncta_b > 0) {
+        A.tasks = (const StreamTask *)P.tasks_b;
+        A.cta_ptr = P.cta_b;
+        k_stream<<<(unsigned)P.ncta_b, ST_THREADS, sm, st>>>(A);
     }
     if (y)
         k_rowsum<float><<<(P.n + 255) / 256, 256, 0, st>>>(P.n, P.leaf_of_row, P.leaf_ptr, P.leaf_off, slots, add0,
                                                            add1, add2, y);
     return pq3d_launch_status();
+}
+
+// Resident CTAs of the streamed kernel on this device (persistent grid size).
+PQ3D_EXPORT int pq3d_stream_ctas(void)
+{
+    int dev = 0, sms = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PQ3D_ERR_CUDA;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return PQ3D_ERR_CUDA;
+    const size_t sm = stream_smem();
+    if (cudaFuncSetAttribute(k_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+        return PQ3D_ERR_CUDA;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stream, ST_THREADS, sm) != cudaSuccess || per <= 0)
+        return PQ3D_ERR_CUDA;
+    return sms * per;
 }
 
 // y (n x 3, FP64, tree order) = K x (+ add_c).  x: deficit in the layout of hm_layout.cuh

@@ -366,18 +366,21 @@ def classify_terms(wS, wD, tol):
     return cls[:len(wS)], cls[len(wS):]
 
 
-def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chunk=32, u_rows=512, stream=False):
+def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chunk=32, u_rows=512, stream=False,
+                            ncta=148):
     """Work items, slot layout and packing records of the mixed storage (code 3):
     FP32 dense items as in the FP32 plan; per low-rank block and term class c
     (FP32, FP16, INT8) the class's own U / V arrays with column groups MIXED_CW[c].
     cls_lists[bi] = (cls_S, cls_D) from classify_terms.  Pure numpy.
 
-    stream=True lays the work out for the bulk-copy kernels (k_v_stream,
-    k_du_stream): one V task per (block, class, column chunk) covering all the
-    class's rows (VItem with q = 0, nr = Q, s = 3 kS | class << 16; chunks of at
-    most STREAM_XMAX columns), and U tasks of at most STREAM_ROWS rows."""
+    stream=True lays the work out for the persistent bulk-copy kernel k_stream:
+    StreamTask lists of phase A (dense tasks of at most STREAM_DENSE_ROWS rows and
+    1,024 columns; V tasks over all rows of one class of one block and at most
+    1,024 columns) and phase B (U tasks of at most STREAM_ROWS rows), each list
+    split over `ncta` persistent CTAs balanced by the bytes they stream, plus
+    one TGather record per low-rank block (the t it gathers into tfull)."""
     if stream:
-        u_rows = min(u_rows, _lib.STREAM_ROWS)
+        return _build_stream_mixed(struct, dense_recs, cls_lists, ncta)
     ditems, slot_rows, slot = _dense_items(dense_recs, 4, dense_recs["off32"], dense_chunk)
     aca_blocks = [b for b in struct.blocks if b.aca]
     u_off, v_off = [0, 0, 0], [0, 0, 0]
@@ -441,6 +444,122 @@ def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chu
              utasks=_rec(utasks, _lib.U_TASK_M), n_ditems=len(ditems), n_vitems=len(vitems), n_utasks=len(utasks),
              n_slots=slot, n_tpart=tp, n_scales=sb, kmax=kmax, u_sizes=u_off, v_sizes=v_off, pack=pack, stream=stream,
              class_terms=counts, alg_bytes=dense_entries * 6 * 4 + lr_bytes + 2 * n * 4 + 3 * n * 8)
+    return A
+
+
+def _balance(tasks, nbytes, ncta):
+    """Tasks grouped by CTA (largest first to the least loaded CTA): (records sorted by
+    CTA, per-CTA ranges of ncta' + 1 entries, ncta' = CTAs with work)."""
+    import heapq
+    if not tasks:
+        return np.zeros(1, dtype=_lib.STREAM_TASK), np.zeros(1, np.int32), 0
+    ncta = max(1, min(int(ncta), len(tasks)))
+    heap = [(0, c) for c in range(ncta)]
+    owner = np.empty(len(tasks), np.int64)
+    for i in np.argsort(-np.asarray(nbytes, np.int64), kind="stable"):
+        load, c = heapq.heappop(heap)
+        owner[i] = c
+        heapq.heappush(heap, (load + int(nbytes[i]), c))
+    order = np.argsort(owner, kind="stable")
+    rec = np.array([tasks[i] for i in order], dtype=_lib.STREAM_TASK)
+    ptr = np.zeros(ncta + 1, np.int32)
+    np.add.at(ptr, owner + 1, 1)
+    return rec, np.cumsum(ptr).astype(np.int32), ncta
+
+
+def _task(kind, **kw):
+    t = dict(off=0, off1=0, off2=0, kind=kind, cls=0, m=0, r0=0, r1=0, g0=0, g1=0, c0=0, out=0, kS3=0, K0=0, K1=0,
+             K2=0, tb=0)
+    t.update(kw)
+    return tuple(t[k] for k in _lib.STREAM_TASK.names)
+
+
+def _build_stream_mixed(struct, dense_recs, cls_lists, ncta):
+    """Task lists of the streamed mixed storage (build_plan_arrays_mixed, stream=True)."""
+    DCOLS, VCOLS = 1024, 1024                  # columns of a dense / V task (x slice in shared memory)
+    n = struct.n
+    ta, ba, tb_, bb, gather = [], [], [], [], []
+    slot_rows, slot = [], 0
+    # dense tasks: (block, column chunk) owns m slots; row ranges share them
+    for i in range(len(dense_recs)):
+        m, nn, r0b, c0 = (int(dense_recs[k][i]) for k in ("m", "n", "r0", "c0"))
+        lead = c0 % 4
+        ng = _cdiv(nn + lead, 4)
+        gch = DCOLS // 4
+        for g0 in range(0, ng, gch):
+            g1 = min(ng, g0 + gch)
+            for r0 in range(0, m, _lib.STREAM_DENSE_ROWS):
+                r1 = min(m, r0 + _lib.STREAM_DENSE_ROWS)
+                ta.append(_task(0, off=int(dense_recs["off32"][i]), m=m, r0=r0, r1=r1, g0=g0, g1=g1, c0=c0 - lead,
+                                out=slot))
+                ba.append((g1 - g0) * (6 * (r1 - r0) * 16 + 32))
+            slot_rows.append((slot, r0b, m))
+            slot += m
+    aca_blocks = [b for b in struct.blocks if b.aca]
+    u_off, v_off = [0, 0, 0], [0, 0, 0]
+    tp = sb = tb = 0
+    pack = []
+    lr_bytes = 0
+    counts = np.zeros((3, 2), np.int64)
+    for bi, b in enumerate(aca_blocks):
+        m, nn = len(b.row.indices), len(b.col.indices)
+        lo, hi = getattr(b, "rows", (0, m))
+        cS, cD = cls_lists[bi]
+        ks = [int((cS == c).sum()) for c in range(3)]
+        kd = [int((cD == c).sum()) for c in range(3)]
+        if sum(ks) + sum(kd) == 0:
+            continue
+        Ks = [_cdiv(ks[c] + kd[c], MIXED_CW[c]) * MIXED_CW[c] for c in range(3)]
+        Qs = [3 * (ks[c] + kd[c]) for c in range(3)]
+        if 3 * sum(Ks) > _lib.STREAM_BUF:
+            raise _lib.Pq3dError("a block's t (%d values) exceeds the stream buffer" % (3 * sum(Ks)))
+        rec_off, rec_voff, rec_tp, rec_nch, rec_sb = [0] * 3, [0] * 3, [0] * 3, [0] * 3, [0] * 3
+        for c in range(3):
+            counts[c] += (ks[c], kd[c])
+            cw = MIXED_CW[c]
+            lr_bytes += Qs[c] * ((hi - lo) + nn) * MIXED_BYTES[c] + (Qs[c] * 4 if c else 0)
+            rec_off[c], rec_voff[c] = u_off[c], v_off[c]
+            if Ks[c] == 0:
+                continue
+            if Qs[c] * 16 > _lib.STREAM_STAGE_BYTES:
+                raise _lib.Pq3dError("a block's term class has %d V rows, more than one stream stage holds" % Qs[c])
+            lead = b.col.start % cw
+            ngv = _cdiv(nn + lead, cw)
+            gch = VCOLS // cw
+            nch = _cdiv(ngv, gch)
+            for ch in range(nch):
+                g0, g1 = ch * gch, min(ngv, (ch + 1) * gch)
+                ta.append(_task(1, off=v_off[c], cls=c, m=Qs[c], g0=g0, g1=g1, c0=b.col.start - lead,
+                                out=tp + ch * Qs[c], kS3=3 * ks[c]))
+                ba.append((g1 - g0) * (Qs[c] * 16 + 8 * cw))
+            rec_tp[c], rec_nch[c] = tp, nch
+            tp += nch * Qs[c]
+            if c:
+                rec_sb[c] = sb
+                sb += Qs[c]
+            u_off[c] += Ks[c] * m * 3
+            v_off[c] += Qs[c] * ngv * cw
+        gather.append((Ks, ks, kd, Qs, rec_tp, rec_nch, rec_sb, tb, 0))
+        for r0 in range(lo, hi, _lib.STREAM_ROWS):
+            r1 = min(hi, r0 + _lib.STREAM_ROWS)
+            tb_.append(_task(2, off=rec_off[0], off1=rec_off[1], off2=rec_off[2], m=m, r0=r0, r1=r1, out=slot - lo,
+                             K0=Ks[0], K1=Ks[1], K2=Ks[2], tb=tb))
+            bb.append(3 * (r1 - r0) * 16 * (Ks[0] // 4 + Ks[1] // 8 + Ks[2] // 16) + 12 * sum(Ks))
+        tb += 3 * sum(Ks)
+        slot_rows.append((slot, b.row.start + lo, hi - lo))
+        for p in (0, 1):
+            pack.append((bi, p, rec_off, rec_voff, ks, kd, Qs, Ks, rec_sb))
+        slot += hi - lo
+    A = _leaf_lists(struct, slot_rows)
+    tasks_a, cta_a, ncta_a = _balance(ta, ba, ncta)
+    tasks_b, cta_b, ncta_b = _balance(tb_, bb, ncta)
+    dense_entries = int(np.sum(dense_recs["m"].astype(np.int64) * dense_recs["n"])) if len(dense_recs) else 0
+    A.update(ditems=_rec([], _lib.DENSE_ITEM), vitems=_rec([], _lib.V_ITEM), utasks=_rec([], _lib.U_TASK_M),
+             n_ditems=0, n_vitems=0, n_utasks=0, n_slots=slot, n_tpart=tp, n_scales=sb, kmax=0, u_sizes=u_off,
+             v_sizes=v_off, pack=pack, stream=True, class_terms=counts,
+             tasks_a=tasks_a, cta_a=cta_a, ncta_a=ncta_a, tasks_b=tasks_b, cta_b=cta_b, ncta_b=ncta_b,
+             gather=_rec(gather, _lib.T_GATHER), n_gather=len(gather), n_tfull=tb,
+             alg_bytes=dense_entries * 6 * 4 + lr_bytes + 2 * n * 4 + 3 * n * 8)
     return A
 
 
@@ -845,10 +964,13 @@ class DeviceHMatrix:
     def _mixed_arrays(self, cls_lists):
         dc, vc, ur = self.shapes("mixed")
         if self.mixed_stream:
-            try:
-                return build_plan_arrays_mixed(self.s, self.dense_recs, cls_lists, dc, vc, ur, stream=True)
-            except _lib.Pq3dError:
-                pass                   # a term class too large for a stream stage: the plain kernels
+            ncta = self.L.pq3d_stream_ctas()
+            if ncta > 0:
+                try:
+                    return build_plan_arrays_mixed(self.s, self.dense_recs, cls_lists, dc, vc, ur, stream=True,
+                                                   ncta=ncta)
+                except _lib.Pq3dError:
+                    pass               # a term class too large for a stream stage: the plain kernels
         return build_plan_arrays_mixed(self.s, self.dense_recs, cls_lists, dc, vc, ur)
 
     def install_mixed(self, tmap, U, V, scales):
@@ -906,6 +1028,16 @@ class DeviceHMatrix:
             hp["status"] = P["status"].data_ptr()
             hp["stream"] = 1 if A.get("stream") else 0
             P["stream"] = bool(A.get("stream"))
+            if P["stream"]:
+                for k in ("tasks_a", "tasks_b", "gather"):
+                    P[k] = dev_rec(A[k])
+                    hp[k] = P[k].data_ptr()
+                for k in ("cta_a", "cta_b"):
+                    P[k] = torch.tensor(A[k], dtype=torch.int32, device=self.dev)
+                    hp[k] = P[k].data_ptr()
+                P["tfull"] = torch.zeros(max(A["n_tfull"], 4), dtype=torch.float32, device=self.dev)
+                hp["tfull"] = P["tfull"].data_ptr()
+                hp["n_gather"], hp["ncta_a"], hp["ncta_b"] = A["n_gather"], A["ncta_a"], A["ncta_b"]
         P["host_plan"] = hp
         P["alg_bytes"] = A["alg_bytes"]
         P["stored_bytes"] = (P["dense"].numel() * P["dense"].element_size() if P["dense"] is not None else 0) + \

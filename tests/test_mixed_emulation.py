@@ -93,7 +93,7 @@ def pack_mixed(st, op, tol, stream=False):
     R = _near_rowabs(st, op)
     W = _weights(st, op, R)
     cls_lists = [classify_terms(wS, wD, tol) for wS, wD in W]
-    A = build_plan_arrays_mixed(st, recs, cls_lists, dense_chunk=2, v_chunk=3, u_rows=40, stream=stream)
+    A = build_plan_arrays_mixed(st, recs, cls_lists, dense_chunk=2, v_chunk=3, u_rows=40, stream=stream, ncta=5)
     dt, fill = (np.float32, np.float16, np.uint8), (0, 0, 128)      # INT8 entries stored as b + 128
     U = [np.full(max(A["u_sizes"][c], 16), fill[c], dt[c]) for c in range(3)]
     V = [np.full(max(A["v_sizes"][c], 16), fill[c], dt[c]) for c in range(3)]
@@ -147,7 +147,87 @@ def _decode(a, cls):
     return a.astype(np.float64) - 128.0 if cls == 2 else a.astype(np.float64)
 
 
+def emulate_stream(st, A, D, U, V, scales, x):
+    """k_stream phase A (dense and V tasks), k_t_gather, k_stream phase B (U tasks), k_rowsum:
+    every task read through the byte ranges its pieces copy, checked against the arrays."""
+    P = x_stride(st.n)
+    STAGE, BUF = 12288, 3072
+    slots = np.zeros(3 * max(A["n_slots"], 1))
+    tpart = np.zeros(max(A["n_tpart"], 1))
+    for name, ncta in (("a", A["ncta_a"]), ("b", A["ncta_b"])):
+        cta = A["cta_" + name]
+        assert cta[0] == 0 and np.all(np.diff(cta) >= 0)
+        if name == "b":
+            # k_t_gather: the blocks' t, contiguous per block
+            tfull = np.zeros(max(A["n_tfull"], 4))
+            for g in A["gather"][:A["n_gather"]]:
+                o = int(g["tb"])
+                for cls in range(3):
+                    K, ks, kd, Q = (int(g[k][cls]) for k in ("K", "kS", "kD", "Q"))
+                    for e in range(3 * K):
+                        c, q = divmod(e, K)
+                        row = c * ks + q if q < ks else (3 * ks + c * kd + q - ks if q < ks + kd else -1)
+                        if row >= 0:
+                            v = sum(tpart[int(g["tp"][cls]) + ch * Q + row] for ch in range(int(g["nch"][cls])))
+                            tfull[o + e] = v * (scales[int(g["sb"][cls]) + row] if cls else 1.0)
+                    o += 3 * K
+                assert o <= A["n_tfull"]
+        for T in A["tasks_" + name][:cta[ncta]]:
+            kind, G = int(T["kind"]), int(T["g1"]) - int(T["g0"])
+            if kind == 0:
+                m, r0, r1, g0 = int(T["m"]), int(T["r0"]), int(T["r1"]), int(T["g0"])
+                R = r1 - r0
+                assert 1 <= R <= 128 and 8 * G <= BUF and 6 * R * 16 <= STAGE and int(T["c0"]) % 4 == 0
+                rr = np.arange(r0, r1)
+                acc = np.zeros((R, 3))
+                for g in range(g0, g0 + G):
+                    for c in range(3):
+                        for sl in range(2):
+                            idx = int(T["off"]) + ((g * 6 + 2 * c + sl) * m + rr)[:, None] * 4 + np.arange(4)
+                            assert idx.max() < len(D)
+                            xv = x[2 * (int(T["c0"]) + g * 4 + np.arange(4)) + sl]
+                            acc[:, c] += D[idx].astype(np.float64) @ xv
+                slots[3 * (int(T["out"]) + rr)[:, None] + np.arange(3)] = acc
+            elif kind == 1:
+                cls, Q, kS3, g0 = int(T["cls"]), int(T["m"]), int(T["kS3"]), int(T["g0"])
+                cw = MIXED_CW[cls]
+                assert Q * 16 <= STAGE and 2 * G * cw <= BUF and int(T["c0"]) % cw == 0
+                for q in range(Q):
+                    plane = 2 if q < kS3 else 3
+                    acc = 0.0
+                    for g in range(g0, g0 + G):
+                        idx = int(T["off"]) + (g * Q + q) * cw + np.arange(cw)
+                        assert idx.max() < len(V[cls])
+                        acc += float(np.dot(_decode(V[cls][idx], cls), x[plane * P + int(T["c0"]) + g * cw + np.arange(cw)]))
+                    tpart[int(T["out"]) + q] = acc
+            else:
+                m, r0, r1, tb = int(T["m"]), int(T["r0"]), int(T["r1"]), int(T["tb"])
+                Ks = (int(T["K0"]), int(T["K1"]), int(T["K2"]))
+                assert 1 <= r1 - r0 <= 256 and 3 * sum(Ks) <= BUF
+                rr = np.arange(r0, r1)
+                acc = np.zeros((len(rr), 3))
+                base = tb
+                for cls, off in enumerate((int(T["off"]), int(T["off1"]), int(T["off2"]))):
+                    cw, K = MIXED_CW[cls], Ks[cls]
+                    for g in range(K // cw):
+                        for c in range(3):
+                            for k in range(cw):
+                                idx = off + ((g * 3 + c) * m + rr) * cw + k
+                                assert idx.max() < len(U[cls])
+                                acc[:, c] += _decode(U[cls][idx], cls) * tfull[base + c * K + g * cw + k]
+                    base += 3 * K
+                slots[3 * (int(T["out"]) + rr)[:, None] + np.arange(3)] = acc
+    y = np.zeros((st.n, 3))
+    for i in range(st.n):
+        lf = A["leaf_of_row"][i]
+        for k in range(A["leaf_ptr"][lf], A["leaf_ptr"][lf + 1]):
+            y[i] += slots[3 * (A["leaf_off"][k] + i):3 * (A["leaf_off"][k] + i) + 3]
+    return y
+
+
 def emulate(st, A, D, U, V, scales, x):
+    if A.get("stream"):
+        return emulate_stream(st, A, D, U, V, scales, x)
     slots = np.zeros(3 * max(A["n_slots"], 1))
     tpart = np.zeros(max(A["n_tpart"], 1))
     for it in A["ditems"][:A["n_ditems"]]:
@@ -162,13 +242,7 @@ def emulate(st, A, D, U, V, scales, x):
                             x[2 * (int(it["c0"]) + g * 4 + t) + s]
         slots[3 * (int(it["slot"]) + rr)[:, None] + np.arange(3)] = acc
     for it in A["vitems"][:A["n_vitems"]]:
-        if A.get("stream"):
-            # k_v_stream: all Q rows of one class; rows below 3 kS use the strike plane
-            cls, kS3 = int(it["s"]) >> 16, int(it["s"]) & 0xffff
-            assert int(it["q"]) == 0 and int(it["nr"]) == int(it["Q"])
-            assert int(it["Q"]) * 16 <= 12288 and (int(it["g1"]) - int(it["g0"])) * MIXED_CW[cls] <= 1024
-        else:
-            cls, kS3 = int(it["s"]) >> 8, None
+        cls, kS3 = int(it["s"]) >> 8, None
         cw = MIXED_CW[cls]
         assert int(it["c0"]) % cw == 0
         Q, q0, nr = int(it["Q"]), int(it["q"]), int(it["nr"])
@@ -222,7 +296,7 @@ def test_mixed_matvec_emulation_within_bound(setup, tol, stream):
     st, op = setup
     A, D, U, V, scales, R, cls = pack_mixed(st, op, tol, stream)
     if stream:
-        assert all(int(T["r1"]) - int(T["r0"]) <= 256 for T in A["utasks"][:A["n_utasks"]])
+        assert A["ncta_a"] > 1 and A["ncta_b"] > 1
     rng = np.random.default_rng(7)
     x1, x2 = rng.standard_normal((2, st.n))
     x = pack_x(x1[st.perm], x2[st.perm], st.n)
