@@ -534,8 +534,11 @@ k_du_mixed(const DenseItem *__restrict__ ditems, int64_t n_ditems, int64_t n_dbl
 //     the column chunks, times the FP16 / INT8 scales) into one contiguous run.
 //   phase B, k_stream (kind 2 U): rows [r0, r1) (<= 256) of a low-rank block; t
 //     piece, then per class and column group the three components' row runs.
-// Consumers map threads to (row, group residue) pairs and reduce the residues at
-// the end of a task, so short row sets keep every thread busy.  All waits are
+// A piece is a flat array of 16-byte units; consumer thread tid owns units tid,
+// tid + 256 and tid + 512 of every piece, whose (group offset, operator or
+// component, row) are the same in all full pieces of a task, so it accumulates
+// in registers, and the owned partial sums are reduced per row in shared memory
+// at the end of the task (fixed order: results are reproducible).  All waits are
 // bounded (ST_SPIN polls); a timeout stores 1 in *status, a task of a size the
 // plan builder never produces stores 2 and is skipped by producer and consumers
 // alike, and the producer waits (bounded) for the copies it issued before exit.
@@ -732,15 +735,6 @@ __device__ __forceinline__ void issue_piece(const StreamArgs &A, const StreamTas
         bulk_g2s(dst + (size_t)c * R * 16, base + (((int64_t)q * 3 + c) * T.m + T.r0) * 16, (unsigned)(R * 16), bar);
 }
 
-template <typename TL>
-__device__ __forceinline__ void consume_v_piece(const unsigned char *st, const float *xs, int Q, int kS3, int ga,
-                                                int gb, int ga0, int q0, int res, int R, float &acc)
-{
-    constexpr int CW = 16 / sizeof(TL);
-    for (int g = ga + ((res - ga) % R + R) % R; g < gb; g += R)     // the piece's groups of residue res
-        acc += dot16<TL>(st + ((size_t)(g - ga0) * Q + q0) * 16, xs + (q0 < kS3 ? 0 : ST_BUF / 2) + g * CW);
-}
-
 __global__ void __launch_bounds__(ST_THREADS, 1) k_stream(StreamArgs A)
 {
     extern __shared__ __align__(128) unsigned char sm[];
@@ -810,118 +804,136 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_stream(StreamArgs A)
             consumers_sync();
         }
         if (T.kind == 0) {
-            // ---- dense: thread -> (row, group residue)
-            const int R = T.r1 - T.r0, RR = ST_CONSUMERS / R, gp = dense_gp(R);
-            const int tr = tid % R, res = tid / R;
-            const bool act = res < RR;
+            // ---- dense: a piece is [gp groups][6 operators][R rows] 16-byte units (the last
+            // piece may hold fewer groups); thread tid owns units tid, tid + 256, tid + 512 of
+            // every piece, so its (group offset, operator, row) are the same in all pieces
+            const int R = T.r1 - T.r0, gp = dense_gp(R), per = 6 * R;
             float acc[3] = {0.f, 0.f, 0.f};
+            int ug[3], uop[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int u = tid + k * ST_CONSUMERS;
+                ug[k] = u / per;
+                uop[k] = (u % per) / R;
+            }
             for (int p = 1; p < np; ++p, ++i) {
                 const int s = i % ST_STAGES;
                 const bool ok = mbar_wait(full + s, (unsigned)(i / ST_STAGES) & 1u);
                 if (!ok) atomicExch(A.status, 1);
-                const int ga = (p - 1) * gp, gb = min(G, ga + gp);
-                if (ok && act) {
-                    const unsigned char *st = stage + (size_t)s * ST_STAGE_BYTES;
-                    for (int g = ga + ((res - ga) % RR + RR) % RR; g < gb; g += RR) {
-                        const float *xv = buf + 8 * g;
-#pragma unroll
-                        for (int c = 0; c < 3; ++c)
-#pragma unroll
-                            for (int sl = 0; sl < 2; ++sl) {
-                                const float4 d = *reinterpret_cast<const float4 *>(
-                                    st + (((size_t)(g - ga) * 6 + 2 * c + sl) * R + tr) * 16);
-                                acc[c] += d.x * xv[sl] + d.y * xv[2 + sl] + d.z * xv[4 + sl] + d.w * xv[6 + sl];
-                            }
-                    }
-                }
-                __syncwarp();
-                if ((tid & 31) == 0) mbar_arrive(empty + s);
-            }
-#pragma unroll
-            for (int c = 0; c < 3; ++c) red[c * ST_CONSUMERS + tid] = act ? acc[c] : 0.f;
-            consumers_sync();
-            if (tid < R) {
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    float v = 0.f;
-                    for (int r = 0; r < RR; ++r) v += red[c * ST_CONSUMERS + r * R + tid];
-                    A.slots[3 * ((int64_t)T.out + T.r0 + tid) + c] = v;
-                }
-            }
-        } else if (T.kind == 1) {
-            // ---- V: thread -> (row q, group residue); rows beyond 256 in a second pass
-            const int Q = T.m, gp = v_gp(Q);
-            const int RR = Q <= ST_CONSUMERS ? ST_CONSUMERS / Q : 1;
-            const int q0 = Q <= ST_CONSUMERS ? tid % Q : tid, res = Q <= ST_CONSUMERS ? tid / Q : 0;
-            const bool act = Q <= ST_CONSUMERS ? res < RR : true;
-            float acc[3] = {0.f, 0.f, 0.f};
-            for (int p = 1; p < np; ++p, ++i) {
-                const int s = i % ST_STAGES;
-                const bool ok = mbar_wait(full + s, (unsigned)(i / ST_STAGES) & 1u);
-                if (!ok) atomicExch(A.status, 1);
-                const int ga = (p - 1) * gp, gb = min(G, ga + gp);
-                if (ok && act) {
+                const int ga = (p - 1) * gp, nu = (min(G, ga + gp) - ga) * per;
+                if (ok) {
                     const unsigned char *st = stage + (size_t)s * ST_STAGE_BYTES;
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
-                        const int q = q0 + k * ST_CONSUMERS;
-                        if (q < Q && (k == 0 || Q > ST_CONSUMERS)) {
-                            if (T.cls == 0) consume_v_piece<float>(st, buf, Q, T.kS3, ga, gb, ga, q, res, RR, acc[k]);
-                            else if (T.cls == 1) consume_v_piece<__half>(st, buf, Q, T.kS3, ga, gb, ga, q, res, RR, acc[k]);
-                            else consume_v_piece<uint8_t>(st, buf, Q, T.kS3, ga, gb, ga, q, res, RR, acc[k]);
+                        const int u = tid + k * ST_CONSUMERS;
+                        if (u < nu) {
+                            const float4 d = *reinterpret_cast<const float4 *>(st + (size_t)u * 16);
+                            const float *xv = buf + 8 * (ga + ug[k]) + (uop[k] & 1);
+                            acc[k] += d.x * xv[0] + d.y * xv[2] + d.z * xv[4] + d.w * xv[6];
                         }
                     }
                 }
                 __syncwarp();
                 if ((tid & 31) == 0) mbar_arrive(empty + s);
             }
-            if (Q <= ST_CONSUMERS) {
-                red[tid] = act ? acc[0] : 0.f;
-                consumers_sync();
-                if (tid < Q) {
-                    float v = 0.f;
-                    for (int r = 0; r < RR; ++r) v += red[r * Q + tid];
-                    A.tpart[T.out + tid] = v;
-                }
-            } else {
+            // per (component, row): the sum over group offsets and slips of the owned units
+            const int full_units = min(G, gp) * per;
 #pragma unroll
-                for (int k = 0; k < 3; ++k)
-                    if (q0 + k * ST_CONSUMERS < Q) A.tpart[T.out + q0 + k * ST_CONSUMERS] = acc[k];
+            for (int k = 0; k < 3; ++k) {
+                const int u = tid + k * ST_CONSUMERS;
+                if (u < full_units) red[u] = acc[k];
             }
-        } else {
-            // ---- U: one thread per row
-            const int R = T.r1 - T.r0;
-            const bool act = tid < R;
+            consumers_sync();
+            for (int e = tid; e < 3 * R; e += ST_CONSUMERS) {
+                const int c = e / R, r = e % R;
+                float v = 0.f;
+                for (int g = 0; g < min(G, gp); ++g)
+                    v += red[(g * 6 + 2 * c) * R + r] + red[(g * 6 + 2 * c + 1) * R + r];
+                A.slots[3 * ((int64_t)T.out + T.r0 + r) + c] = v;
+            }
+        } else if (T.kind == 1) {
+            // ---- V: a piece is [gp groups][Q rows] units; thread tid owns units tid + 256 k
+            const int Q = T.m, gp = v_gp(Q), CW = cw_of(T.cls);
             float acc[3] = {0.f, 0.f, 0.f};
-            const int n0 = T.K0 / 4, n1 = T.K1 / 8;
+            int ug[3], uq[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int u = tid + k * ST_CONSUMERS;
+                ug[k] = u / Q;
+                uq[k] = u % Q;
+            }
             for (int p = 1; p < np; ++p, ++i) {
                 const int s = i % ST_STAGES;
                 const bool ok = mbar_wait(full + s, (unsigned)(i / ST_STAGES) & 1u);
                 if (!ok) atomicExch(A.status, 1);
-                if (ok && act) {
-                    const unsigned char *st = stage + (size_t)s * ST_STAGE_BYTES + (size_t)tid * 16;
-                    const int q = p - 1;
-                    if (q < n0) {
+                const int ga = (p - 1) * gp, nu = (min(G, ga + gp) - ga) * Q;
+                if (ok) {
+                    const unsigned char *st = stage + (size_t)s * ST_STAGE_BYTES;
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) acc[c] += dot16<float>(st + (size_t)c * R * 16, buf + c * T.K0 + q * 4);
-                    } else if (q < n0 + n1) {
-                        const float *tc = buf + 3 * T.K0;
-#pragma unroll
-                        for (int c = 0; c < 3; ++c)
-                            acc[c] += dot16<__half>(st + (size_t)c * R * 16, tc + c * T.K1 + (q - n0) * 8);
-                    } else {
-                        const float *tc = buf + 3 * (T.K0 + T.K1);
-#pragma unroll
-                        for (int c = 0; c < 3; ++c)
-                            acc[c] += dot16<uint8_t>(st + (size_t)c * R * 16, tc + c * T.K2 + (q - n0 - n1) * 16);
+                    for (int k = 0; k < 3; ++k) {
+                        const int u = tid + k * ST_CONSUMERS;
+                        if (u < nu) {
+                            const float *xv = buf + (uq[k] < T.kS3 ? 0 : ST_BUF / 2) + (ga + ug[k]) * CW;
+                            if (T.cls == 0) acc[k] += dot16<float>(st + (size_t)u * 16, xv);
+                            else if (T.cls == 1) acc[k] += dot16<__half>(st + (size_t)u * 16, xv);
+                            else acc[k] += dot16<uint8_t>(st + (size_t)u * 16, xv);
+                        }
                     }
                 }
                 __syncwarp();
                 if ((tid & 31) == 0) mbar_arrive(empty + s);
             }
-            if (act) {
+            const int full_units = min(G, gp) * Q;
 #pragma unroll
-                for (int c = 0; c < 3; ++c) A.slots[3 * ((int64_t)T.out + T.r0 + tid) + c] = acc[c];
+            for (int k = 0; k < 3; ++k) {
+                const int u = tid + k * ST_CONSUMERS;
+                if (u < full_units) red[u] = acc[k];
+            }
+            consumers_sync();
+            for (int q = tid; q < Q; q += ST_CONSUMERS) {
+                float v = 0.f;
+                for (int g = 0; g < min(G, gp); ++g) v += red[g * Q + q];
+                A.tpart[T.out + q] = v;
+            }
+        } else {
+            // ---- U: a piece is [3 components][R rows] units; thread tid owns units tid + 256 k
+            const int R = T.r1 - T.r0;
+            float acc[3] = {0.f, 0.f, 0.f};
+            int uc[3], ur[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int u = tid + k * ST_CONSUMERS;
+                uc[k] = u / R;
+                ur[k] = u % R;
+            }
+            const int n0 = T.K0 / 4, n1 = T.K1 / 8;
+            for (int p = 1; p < np; ++p, ++i) {
+                const int s = i % ST_STAGES;
+                const bool ok = mbar_wait(full + s, (unsigned)(i / ST_STAGES) & 1u);
+                if (!ok) atomicExch(A.status, 1);
+                if (ok) {
+                    const unsigned char *st = stage + (size_t)s * ST_STAGE_BYTES;
+                    const int q = p - 1;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const int u = tid + k * ST_CONSUMERS;
+                        if (u < 3 * R) {
+                            if (q < n0) acc[k] += dot16<float>(st + (size_t)u * 16, buf + uc[k] * T.K0 + q * 4);
+                            else if (q < n0 + n1)
+                                acc[k] += dot16<__half>(st + (size_t)u * 16, buf + 3 * T.K0 + uc[k] * T.K1 + (q - n0) * 8);
+                            else
+                                acc[k] += dot16<uint8_t>(st + (size_t)u * 16,
+                                                         buf + 3 * (T.K0 + T.K1) + uc[k] * T.K2 + (q - n0 - n1) * 16);
+                        }
+                    }
+                }
+                __syncwarp();
+                if ((tid & 31) == 0) mbar_arrive(empty + s);
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int u = tid + k * ST_CONSUMERS;
+                if (u < 3 * R) A.slots[3 * ((int64_t)T.out + T.r0 + ur[k]) + uc[k]] = acc[k];
             }
         }
         consumers_sync();      // buf and red are reused by the next task
