@@ -393,6 +393,20 @@ k_u(const UTask *__restrict__ tasks, const TL *__restrict__ U, const TA *__restr
 }
 
 // ------------------------------------------------------------------ mixed storage
+// Resident CTAs per SM the register allocation of k_v_mixed / k_du_mixed is held to
+// (measured on B200 at 60k, mixed matvec: 6 and 5 give 0.483 ms against 0.672 ms for
+// the compiler's own choice at one CTA per SM and 0.499 ms for 5 and 5; both kernels are
+// latency-bound streams, so occupancy matters more than a few spilled registers).
+#ifndef PQ3D_VMIX_MINB
+#define PQ3D_VMIX_MINB 6
+#endif
+#ifndef PQ3D_UMIX_MINB
+#define PQ3D_UMIX_MINB 5
+#endif
+#ifndef PQ3D_UMIX_UNROLL
+#define PQ3D_UMIX_UNROLL 2
+#endif
+constexpr int kUmixUnroll = PQ3D_UMIX_UNROLL;     // column groups of a U row in flight
 // Storage code 3: FP32 dense near field; each low-rank block's ACA terms split
 // into three classes stored as FP32, FP16 and INT8 (class arrays U_c, V_c in
 // the layouts of hm_layout.cuh with CW = 4, 8, 16).  FP16 and INT8 columns of U
@@ -416,24 +430,31 @@ __device__ __forceinline__ void u_row_class(const TL *__restrict__ Ub, int m, in
     const int ng = K / CW;
     const TL *p = Ub + (int64_t)r * CW;                   // [group][comp][row][CW]
     const int64_t cstride = (int64_t)m * CW, gstride = 3 * cstride;
-#pragma unroll 2
+#pragma unroll kUmixUnroll
     for (int g = 0; g < ng; ++g) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             Vec16<TL> d = ld_stream(p + c * cstride);
-            float tv[CW];
-            smem_vec<float, CW>(ts + c * K + g * CW, tv);
+            const float4 *t4 = reinterpret_cast<const float4 *>(ts + c * K + g * CW);
             if constexpr (std::is_same<TL, uint8_t>::value) {
+                // t read four values at a time: 4 live registers instead of 16
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    acc[c] += i8_at<0>(d.w[k]) * tv[4 * k];
-                    acc[c] += i8_at<1>(d.w[k]) * tv[4 * k + 1];
-                    acc[c] += i8_at<2>(d.w[k]) * tv[4 * k + 2];
-                    acc[c] += i8_at<3>(d.w[k]) * tv[4 * k + 3];
+                    const float4 tv = t4[k];
+                    acc[c] += i8_at<0>(d.w[k]) * tv.x;
+                    acc[c] += i8_at<1>(d.w[k]) * tv.y;
+                    acc[c] += i8_at<2>(d.w[k]) * tv.z;
+                    acc[c] += i8_at<3>(d.w[k]) * tv.w;
                 }
             } else {
 #pragma unroll
-                for (int k = 0; k < CW; ++k) acc[c] += tof(d.v[k]) * tv[k];
+                for (int k = 0; k < CW / 4; ++k) {
+                    const float4 tv = t4[k];
+                    acc[c] += tof(d.v[4 * k]) * tv.x;
+                    acc[c] += tof(d.v[4 * k + 1]) * tv.y;
+                    acc[c] += tof(d.v[4 * k + 2]) * tv.z;
+                    acc[c] += tof(d.v[4 * k + 3]) * tv.w;
+                }
             }
         }
         p += gstride;
@@ -478,7 +499,7 @@ __device__ __forceinline__ void u_task_mixed(const UTaskM &T, const float *__res
 }
 
 // V items of all three classes, one warp each (the class picks the element type).
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, PQ3D_VMIX_MINB)
 k_v_mixed(const VItem *__restrict__ vitems, int64_t n_vitems, const float *__restrict__ V32,
           const __half *__restrict__ V16, const uint8_t *__restrict__ V8, const float *__restrict__ x, int xstride,
           float *__restrict__ tpart)
@@ -495,7 +516,7 @@ k_v_mixed(const VItem *__restrict__ vitems, int64_t n_vitems, const float *__res
 
 // Dense items, then the mixed U tasks (programmatic dependent launch after k_v_mixed,
 // as k_du after k_dense_v).
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, PQ3D_UMIX_MINB)
 k_du_mixed(const DenseItem *__restrict__ ditems, int64_t n_ditems, int64_t n_dblocks,
            const UTaskM *__restrict__ tasks, const float *__restrict__ D, const float *__restrict__ U32,
            const __half *__restrict__ U16, const uint8_t *__restrict__ U8, const float *__restrict__ x,

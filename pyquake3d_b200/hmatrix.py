@@ -623,7 +623,7 @@ class DeviceHMatrix:
         compiled library (the values its H-matrix assembly uses).  mixed_tol: the
         term-class tolerance of the "mixed" storage (classify_terms)."""
         self.mixed_tol = float(mixed_tol)
-        self.mixed_stream = True       # mixed storage: bulk-copy (streamed) low-rank kernels
+        self.mixed_stream = False      # mixed storage: True selects the bulk-copy (streamed) kernels
         self.use_plan_cache = True
         import torch
         self.torch = torch
