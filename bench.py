@@ -248,14 +248,16 @@ def accuracy_study(sim, op, nrep, precisions=("bf16",), marks=(50, 100, 200, 500
     return out
 
 
-def vmode_study(sim, op, nsteps):
-    """V-mode steps/s with the FP32 and FP64 operators, plain Newton (undamped start)
-    vs the MLP start, and the Newton iteration counts.  The MLP is trained first on
-    solves logged from a short plain run of the same fault."""
+def vmode_study(sim, op, nsteps, prec="fp32"):
+    """V-mode steps/s and Newton iteration counts for every start of the slip-rate
+    solve -- the previous rate (seed 0), the undamped bound (seed 1), the MLP (seed 2)
+    and the gated MLP (seed 3) -- with the `prec` operator, and plain Newton with the
+    FP64 operator.  The MLP is trained first on solves logged from a short plain run
+    of the same fault."""
     import torch
     from pyquake3d_b200.vmode import MLPTrainer, VStepper
     out = {}
-    logger = VStepper(sim, op, "fp32", seed_mode=1, log_cap=1 << 20)
+    logger = VStepper(sim, op, prec, seed_mode=1, log_cap=1 << 20)
     logger.run(20, chunk=4)
     data = logger.samples()
     t0 = time.perf_counter()
@@ -265,8 +267,9 @@ def vmode_study(sim, op, nsteps):
     out["mlp"] = {"samples": int(data.shape[0]), "epochs": 15, "train_s": round(time.perf_counter() - t0, 2),
                   "loss_first": hist[0], "loss_last": hist[-1]}
     del logger
-    for prec, mode in (("fp32", 1), ("fp32", 2), ("fp64", 1)):
-        st = VStepper(sim, op, prec, seed_mode=mode, mlp_params=tr.P if mode == 2 else None)
+    names = {0: "prev", 1: "newton", 2: "mlp", 3: "mlp_gated"}
+    for prc, mode in ((prec, 0), (prec, 1), (prec, 2), (prec, 3), ("fp64", 1)):
+        st = VStepper(sim, op, prc, seed_mode=mode, mlp_params=tr.P if mode >= 2 else None)
         st.run(5, chunk=2)                      # warm-up steps
         st.reset_stats()
         c0 = st.ctrl.cpu().numpy().copy()
@@ -278,12 +281,36 @@ def vmode_study(sim, op, nsteps):
         torch.cuda.synchronize()
         secs = e0.elapsed_time(e1) / 1e3
         steps = int(c[8] - c0[8])
-        out["%s_%s" % (prec, "mlp" if mode == 2 else "newton")] = {
+        out["%s_%s" % (prc, names[mode])] = {
             "steps_per_s": steps / secs, "steps": steps, "attempts": int(c[10] - c0[10]),
             "matvecs_per_step": 6 * (c[10] - c0[10]) / max(steps, 1), "sim_time_s": float(c[2]),
             "newton": st.newton_stats()}
         del st
-    out["mixed_mlp_vs_fp64_newton"] = out["fp32_mlp"]["steps_per_s"] / out["fp64_newton"]["steps_per_s"]
+    out["mixed_mlp_vs_fp64_newton"] = out["%s_mlp_gated" % prec]["steps_per_s"] / out["fp64_newton"]["steps_per_s"]
+    best = max(out["%s_prev" % prec]["steps_per_s"], out["%s_newton" % prec]["steps_per_s"])
+    out["mlp_gated_vs_best_classical"] = out["%s_mlp_gated" % prec]["steps_per_s"] / best
+    return out
+
+
+def vmode_config3(nsteps):
+    """Config 3: curved120k (the 60k geometry refined, a - b from a seeded Gaussian field
+    in [-0.006, 0.006], sigma_n in [20, 80] MPa) in V-mode with the gated MLP start:
+    steps/s and Newton statistics against the classical starts."""
+    import gc
+    import torch
+    from pyquake3d_b200 import QDsim, read_mshV2
+    set_case("curved120k")
+    msh, para = make_case(0)
+    set_case("curved60k")
+    nodes, tris = read_mshV2(msh)
+    sim = QDsim(tris, nodes, para, precision="mixed")
+    sim.tree_block.want = ("fp64", "mixed")
+    op = sim.tree_block.op()
+    out = vmode_study(sim, op, nsteps, prec="mixed")
+    out["triangles"] = int(op.n)
+    del op, sim
+    gc.collect()
+    torch.cuda.empty_cache()
     return out
 
 
@@ -507,6 +534,7 @@ def main():
     ap.add_argument("--case", default=CASE, help="workload (profiling uses a smaller one)")
     ap.add_argument("--no-vmode", action="store_true", help="skip the V-mode study")
     ap.add_argument("--vmode-steps", type=int, default=60)
+    ap.add_argument("--vmode120-steps", type=int, default=30, help="config 3 (curved120k) V-mode study; 0 skips")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 32-fault ensemble study")
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--accuracy-steps", type=int, default=500,
@@ -648,7 +676,13 @@ def main():
     # trained on the run's own solves (hand-written kernels)
     vmode = None
     if not args.no_vmode:
-        vmode = vmode_study(sim, op, args.vmode_steps)
+        vmode = vmode_study(sim, op, args.vmode_steps, prec="mixed")
+
+    # config 3 (curved120k, heterogeneous friction) in V-mode with the gated MLP, on an
+    # operator of its own; the 60k steppers stay resident beside it
+    vmode120 = None
+    if not args.no_vmode and args.vmode120_steps > 0 and world == 1:
+        vmode120 = vmode_config3(args.vmode120_steps)
 
     # end to end through the reference call surface (QDsim.simu_forward) with the
     # reference main loop's per-step host traffic
@@ -764,6 +798,7 @@ def main():
         "accuracy_vs_fp64": accuracy,
         "fp64_pinned_to_oracle": pinned,
         "vmode": vmode,
+        "vmode_curved120k": vmode120,
         "ensemble": ensemble,
         "gf_assembly": gf,
         "sim": {"time_s": float(hist[-1, 2]), "last_dt": float(hist[-1, 0]), "rejects": int(hist[:, 5].sum())},

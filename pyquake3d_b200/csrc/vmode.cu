@@ -128,6 +128,11 @@ __device__ inline bool newton(double S, double lk, double tol, int maxit, double
     return false;
 }
 
+// First-step correction (in z = asinh(|V| e^{psi/a} / 2V0)) above which the gated
+// mode consults the network: the previous stage's rate is then off by more than a
+// factor e.
+constexpr double MLP_GATE = 1.0;
+
 __device__ inline Solve vsolve(double tq, double sig, double psi, double a, double b, double V0, double eta,
                                double Vprev, int mode, const float *P, double tol, int maxit, float *logx,
                                unsigned long long *logn, long long logcap)
@@ -145,7 +150,46 @@ __device__ inline Solve vsolve(double tq, double sig, double psi, double a, doub
         const double dz = 0.5 * e * (1.0 - q) / (1.0 + 0.5 * e * (1.0 + q));
         easy = dz <= tol * fmax(1.0, S);
     }
-    if (mode == 2 && P && easy) {
+    if (mode == 3 && P) {
+        // Gated network start: the previous-rate start (mode 0) takes its first Newton
+        // step; only when that step's correction exceeds MLP_GATE in z (the rate is off
+        // by more than a factor e^MLP_GATE) is the network's start evaluated, and Newton
+        // goes on from whichever start has the smaller residual.  Every residual
+        // evaluation counts as an iteration; the bracketed solve stays the fallback.
+        double z0 = S;
+        if (Vprev != 0.0) {
+            const double L = log(fabs(Vprev) / (2.0 * V0)) + psi / a;
+            z0 = L > 20.0 ? L + 0.6931471805599453 : asinh(exp(L));
+            z0 = z0 < 0.0 ? 0.0 : (z0 > S ? S : z0);
+        }
+        const double e0 = exp(lk + z0), q0 = exp(-2.0 * z0);
+        const double F0 = z0 + 0.5 * e0 * (1.0 - q0) - S;
+        const double dz0 = F0 / (1.0 + 0.5 * e0 * (1.0 + q0));
+        double z1 = z0 - dz0;
+        z1 = z1 < 0.0 ? 0.0 : (z1 > S ? S : z1);
+        r.iters = 1;
+        if (fabs(z1 - z0) <= tol * fmax(1.0, z0)) {
+            z = z1;
+        } else {
+            z = z1;
+            if (fabs(dz0) > MLP_GATE) {
+                float f[5];
+                mlp_features(S, lk, a, b, sig, f);
+                const double zm = S / (1.0 + exp(-(double)mlp_eval(P, f)));
+                const double Fm = zm + 0.5 * exp(lk + zm) * (1.0 - exp(-2.0 * zm)) - S;
+                const double F1 = z1 + 0.5 * exp(lk + z1) * (1.0 - exp(-2.0 * z1)) - S;
+                r.iters += 2;
+                if (fabs(Fm) < fabs(F1)) z = zm;
+            }
+            ok = newton(S, lk, tol, maxit, z, r.iters);
+            const double e = exp(lk + z), res = fabs(z + 0.5 * e * (1.0 - exp(-2.0 * z)) - S);
+            if (!ok || res > 1e-10 * (1.0 + S)) {
+                r.fallback = true;
+                z = S;
+                ok = newton(S, lk, tol, maxit, z, r.iters);
+            }
+        }
+    } else if (mode == 2 && P && easy) {
         z = S;
         r.iters = 1;
     } else if (mode == 2 && P) {
@@ -205,7 +249,7 @@ __global__ void __launch_bounds__(VM_THREADS) k_vmode_stage(VArgs A, int s)
     __shared__ int s_last;
     // MLP parameters are read in place through the read-only cache: only solves that
     // fail the undamped-start test touch them, and a warp's lanes read the same weight.
-    const bool use_mlp = A.seed_mode == 2 && A.mlp;
+    const bool use_mlp = (A.seed_mode == 2 || A.seed_mode == 3) && A.mlp;
     const float *__restrict__ P = A.mlp;
     const int n = A.n;
     const double h = A.ctrl[0], t0 = A.ctrl[2];

@@ -8,6 +8,9 @@ and operators.  The initial guess of every Newton solve is one of
   seed 0: the element's previous rate        seed 1: the undamped bound z = S
   seed 2: the MLP (trained here on the stepper's own converged solves), consulted
           only where one Newton step from z = S does not already converge
+  seed 3: the gated MLP: the previous rate takes the first Newton step; the MLP
+          is consulted only when that step's correction exceeds 1 in z, and
+          Newton goes on from the start with the smaller residual
 and plain Newton (from z = S) stays the fallback and the judge: an MLP start
 whose residual is above 1e-10 after 8 steps is discarded.
 """
