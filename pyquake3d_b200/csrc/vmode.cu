@@ -44,6 +44,7 @@ struct VArgs {
     long long log_cap;
     int n, x_fp32, seed_mode, newton_max;
     double V0, eta, reltol, atol, newton_tol;
+    double mlp_gate;      // seed 3: first-step correction (in z) above which the MLP is consulted
 };
 
 __device__ const double kC[7] = {0.0, 1.0 / 5, 3.0 / 10, 4.0 / 5, 8.0 / 9, 1.0, 1.0};
@@ -128,13 +129,8 @@ __device__ inline bool newton(double S, double lk, double tol, int maxit, double
     return false;
 }
 
-// First-step correction (in z = asinh(|V| e^{psi/a} / 2V0)) above which the gated
-// mode consults the network: the previous stage's rate is then off by more than a
-// factor e.
-constexpr double MLP_GATE = 1.0;
-
 __device__ inline Solve vsolve(double tq, double sig, double psi, double a, double b, double V0, double eta,
-                               double Vprev, int mode, const float *P, double tol, int maxit, float *logx,
+                               double Vprev, int mode, const float *P, double gate, double tol, int maxit, float *logx,
                                unsigned long long *logn, long long logcap)
 {
     const double S = fabs(tq) / (a * sig);
@@ -151,35 +147,27 @@ __device__ inline Solve vsolve(double tq, double sig, double psi, double a, doub
         easy = dz <= tol * fmax(1.0, S);
     }
     if (mode == 3 && P) {
-        // Gated network start: the previous-rate start (mode 0) takes its first Newton
-        // step; only when that step's correction exceeds MLP_GATE in z (the rate is off
-        // by more than a factor e^MLP_GATE) is the network's start evaluated, and Newton
-        // goes on from whichever start has the smaller residual.  Every residual
-        // evaluation counts as an iteration; the bracketed solve stays the fallback.
-        double z0 = S;
-        if (Vprev != 0.0) {
-            const double L = log(fabs(Vprev) / (2.0 * V0)) + psi / a;
-            z0 = L > 20.0 ? L + 0.6931471805599453 : asinh(exp(L));
-            z0 = z0 < 0.0 ? 0.0 : (z0 > S ? S : z0);
-        }
-        const double e0 = exp(lk + z0), q0 = exp(-2.0 * z0);
-        const double F0 = z0 + 0.5 * e0 * (1.0 - q0) - S;
-        const double dz0 = F0 / (1.0 + 0.5 * e0 * (1.0 + q0));
-        double z1 = z0 - dz0;
-        z1 = z1 < 0.0 ? 0.0 : (z1 > S ? S : z1);
+        // Gated network start.  The undamped start z = S takes its first Newton step
+        // (the "easy" test above); when that step's correction is at most `gate` in z
+        // the solve goes on with plain Newton from there -- the usual case away from
+        // nucleation, where it converges in a step or two -- and only a larger
+        // correction (strong radiation damping) evaluates the network, whose start Newton
+        // then refines.  The step from z = S counts as an iteration either way; the
+        // bracketed solve stays the fallback.
+        const double e0 = exp(lk + S), q0 = exp(-2.0 * S);
+        const double dz0 = 0.5 * e0 * (1.0 - q0) / (1.0 + 0.5 * e0 * (1.0 + q0));
         r.iters = 1;
-        if (fabs(z1 - z0) <= tol * fmax(1.0, z0)) {
-            z = z1;
+        double z1 = S - dz0;
+        z1 = z1 < 0.0 ? 0.0 : z1;
+        if (dz0 <= tol * fmax(1.0, S)) {
+            z = S;
         } else {
-            z = z1;
-            if (fabs(dz0) > MLP_GATE) {
+            if (dz0 > gate) {
                 float f[5];
                 mlp_features(S, lk, a, b, sig, f);
-                const double zm = S / (1.0 + exp(-(double)mlp_eval(P, f)));
-                const double Fm = zm + 0.5 * exp(lk + zm) * (1.0 - exp(-2.0 * zm)) - S;
-                const double F1 = z1 + 0.5 * exp(lk + z1) * (1.0 - exp(-2.0 * z1)) - S;
-                r.iters += 2;
-                if (fabs(Fm) < fabs(F1)) z = zm;
+                z = S / (1.0 + exp(-(double)mlp_eval(P, f)));
+            } else {
+                z = z1;
             }
             ok = newton(S, lk, tol, maxit, z, r.iters);
             const double e = exp(lk + z), res = fabs(z + 0.5 * e * (1.0 - exp(-2.0 * z)) - S);
@@ -272,9 +260,9 @@ __global__ void __launch_bounds__(VM_THREADS) k_vmode_stage(VArgs A, int s)
         const double tq2 = A.tq2[i] - A.mv[3 * i + 1] + A.shear_loading[i] * ts;
         const double sig = A.sig0[i] + A.mv[3 * i + 2] + A.normal_loading[i] * ts;
         const Solve r1 = vsolve(tq1, sig, ys[2], a, b, A.V0, A.eta, A.V[i], A.seed_mode, use_mlp ? P : nullptr,
-                                A.newton_tol, A.newton_max, A.log_x, A.log_n, A.log_cap);
+                                A.mlp_gate, A.newton_tol, A.newton_max, A.log_x, A.log_n, A.log_cap);
         const Solve r2 = vsolve(tq2, sig, ys[2], a, b, A.V0, A.eta, A.V[n + i], A.seed_mode, use_mlp ? P : nullptr,
-                                A.newton_tol, A.newton_max, A.log_x, A.log_n, A.log_cap);
+                                A.mlp_gate, A.newton_tol, A.newton_max, A.log_x, A.log_n, A.log_cap);
         A.V[i] = r1.V;
         A.V[n + i] = r2.V;
         its = r1.iters + r2.iters;

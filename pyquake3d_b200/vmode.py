@@ -8,15 +8,19 @@ and operators.  The initial guess of every Newton solve is one of
   seed 0: the element's previous rate        seed 1: the undamped bound z = S
   seed 2: the MLP (trained here on the stepper's own converged solves), consulted
           only where one Newton step from z = S does not already converge
-  seed 3: the gated MLP: the previous rate takes the first Newton step; the MLP
-          is consulted only when that step's correction exceeds 1 in z, and
-          Newton goes on from the start with the smaller residual
+  seed 3: the gated MLP: the undamped start takes the first Newton step; plain
+          Newton goes on when its correction is at most MLP_GATE in z, and only
+          larger corrections (strong radiation damping) evaluate the MLP
 and plain Newton (from z = S) stays the fallback and the judge: an MLP start
 whose residual is above 1e-10 after 8 steps is discarded.
 """
 import ctypes
 
 import numpy as np
+
+# seed 3: first Newton correction from the undamped start (in z) above which the MLP
+# proposes the start; smaller ones converge in a step or two of plain Newton
+MLP_GATE = 0.5
 
 from . import _lib
 from ._lib import check, ptr, stream_ptr
@@ -26,7 +30,7 @@ VARGS_PTRS = ["y0", "k", "y5", "mv", "tq1", "tq2", "sig0", "a", "b", "dc", "f0",
 VARGS = np.dtype([(p, "u8") for p in VARGS_PTRS] + [("log_cap", "i8"), ("n", "i4"), ("x_fp32", "i4"),
                                                     ("seed_mode", "i4"), ("newton_max", "i4"), ("V0", "f8"),
                                                     ("eta", "f8"), ("reltol", "f8"), ("atol", "f8"),
-                                                    ("newton_tol", "f8")], align=True)
+                                                    ("newton_tol", "f8"), ("mlp_gate", "f8")], align=True)
 # control block: [0] h of the next attempt, [1] last accepted h, [2] time, [3] consecutive rejects,
 # [4] status, [8] accepted steps, [9] rejects, [10] attempts, [11] last attempt accepted, [12] dtnext, [13] E
 MLP_NP = 4609
@@ -177,6 +181,7 @@ class VStepper:
         A["seed_mode"] = seed_mode
         A["newton_max"] = newton_max
         A["V0"], A["eta"], A["reltol"], A["atol"], A["newton_tol"] = sim.V0, eta, reltol, atol, 1e-12
+        A["mlp_gate"] = MLP_GATE
         self.args = A
         self.started = False
 

