@@ -14,6 +14,10 @@ plan.
 
     python -m pyquake3d_b200.autotune --case curved60k --precisions fp32,mixed,fp64 \
         [--out plan_cache.json]
+
+With --time-only it builds the case, times one H-matvec per storage with the plan
+cache's shapes (3 warm-up and --reps timed launches) and prints the times: the
+driver of the matvec profiles.
 """
 import argparse
 import json
@@ -75,6 +79,7 @@ def main():
     ap.add_argument("--precisions", default="fp32,mixed,fp64,bf16")
     ap.add_argument("--out", default=None, help="plan cache to update (default: the package's plan_cache.json)")
     ap.add_argument("--reps", type=int, default=30)
+    ap.add_argument("--time-only", action="store_true", help="time the matvec with the cached shapes, no tuning")
     args = ap.parse_args()
     import torch
     from . import meshgen
@@ -88,6 +93,18 @@ def main():
     sim = QDsim(tris, nodes, para, precision=precs[0])
     sim.tree_block.want = tuple(sorted(set(["fp64"] + precs)))
     op = sim.tree_block.op()
+    if args.time_only:
+        for p in precs:
+            x = op.new_x(p)
+            x.copy_(torch.randn_like(x) * 1e-9)
+            t = time_matvec(op, p, x, args.reps)
+            P = op.plan(p)
+            out = dict(case=args.case, n=int(op.n), precision=p, shapes=op.shapes(p), us=round(1e6 * t, 1),
+                       alg_bytes=int(P["alg_bytes"]), GBs=round(P["alg_bytes"] / t / 1e9, 1))
+            if p == "mixed":
+                out["terms_fp32_fp16_int8"] = [int(sum(c)) for c in P["mixed"]["class_terms"]]
+            print(json.dumps(out))
+        return
     op.use_plan_cache = False            # tune from the built-in defaults
     gpu = torch.cuda.get_device_name(op.dev)
     out = args.out or PLAN_CACHE

@@ -83,3 +83,41 @@ def test_ensemble_mixed_precision_on_fp64_steps(files):
     for f in range(ref.M):
         a, b = mix.get("slip", f), ref.get("slip", f)
         assert np.linalg.norm(a - b) <= 1e-6 * np.linalg.norm(b), f
+
+
+def test_full_32_fault_deck_fp32_and_mixed_within_target_or_chaos_floor(tmp_path_factory):
+    """The benchmark's config-4 deck (32 planar faults of U[2000, 20000] triangles, seed 4,
+    dips U[20, 90] degrees, seeded friction), 100 steps: the FP32 and mixed-storage
+    ensembles on the FP64 ensemble's step sizes (dt replay).  Each fault's slip error
+    must stay within the 1e-5 target, or within twice that fault's FP64 chaos floor --
+    the same error between two FP64 runs whose initial shear tractions differ by a
+    relative 1e-12 -- where the fault itself amplifies any perturbation beyond the
+    target (an accelerating fault: no storage short of the FP64 run reproduces it)."""
+    from pyquake3d_b200 import QDsim, read_mshV2
+    from pyquake3d_b200.ensemble import Ensemble
+    from pyquake3d_b200.meshgen import ensemble_faults
+    files = ensemble_faults(str(tmp_path_factory.mktemp("deck32")), n_faults=32, seed=4, lo=2000, hi=20000, edge=0.5)
+    sims = []
+    for msh, para in files:
+        nodes, tris = read_mshV2(msh)
+        sims.append(QDsim(tris, nodes, para, precision="fp32"))
+    nrep = 100
+    h0 = [s.htry for s in sims]
+    E64 = Ensemble(sims, precision="fp64", want=("fp64", "fp32", "mixed"))
+    h = E64.run(nrep, h0)
+    runs = {}
+    for name, prec in (("fp32", "fp32"), ("mixed", "mixed"), ("floor", "fp64")):
+        R = Ensemble(sims, precision=prec, share=E64)
+        if name == "floor":
+            R.t["Tt1o"].mul_(1.0 + 1e-12)
+        R.set_replay(torch.tensor(h[:, :, 0], device=R.op.dev))
+        R.run(nrep, h0)
+        runs[name] = R
+    worst = {}
+    for f in range(len(sims)):
+        b = E64.get("slip", f)
+        e = {k: float(np.linalg.norm(R.get("slip", f) - b) / np.linalg.norm(b)) for k, R in runs.items()}
+        for k in ("fp32", "mixed"):
+            assert e[k] <= max(1e-5, 2.0 * e["floor"]), (f, e)
+            worst[k] = max(worst.get(k, 0.0), e[k])
+    assert worst["fp32"] <= 1e-4 and worst["mixed"] <= 1e-4, worst
