@@ -20,8 +20,12 @@ A step = one H-matvec of the slip-rate deficit + one fused DP5(4) step kernel
               port) on the same operator, bounded sample, on the host cores
 --impl reference runs only that CPU arm (all host cores, the reference's MPI
 block split emulated with worker processes) and prints its own line.
-Multi-GPU (torchrun): every rank simulates its own fault replica (independent
-ensemble members, no data-path collective); value = sum over ranks.
+Multi-GPU (torchrun): the one fault row-partitioned over the ranks (strong
+scaling; run_partition: one all-gather of the deficit per step, one max
+all-reduce per attempt, the controller on the device, CUDA-graph replays);
+value = steps of that fault per second.  --parallelism replicas runs one fault
+per rank instead (value = sum over ranks).  --parallelism partition on one GPU
+runs the partitioned path with a single rank.
 """
 import argparse
 import json
@@ -135,15 +139,30 @@ class Clocks:
                                        "-i", str(gpu_index)], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+        # the sampler's first row before the timed region starts (nvidia-smi takes a
+        # few hundred ms to come up); rows from then on are the region's
+        self.n0 = 0
+        t0 = time.time()
+        while self.p is not None and time.time() - t0 < 5.0 and self.p.poll() is None:
+            self.n0 = len(self._rows())
+            if self.n0:
+                break
+            time.sleep(0.05)
+
+    def _rows(self):
+        self.f.flush()
+        return [l.strip().split(", ") for l in open(self.f.name) if l.strip()]
 
     def stop(self):
         if self.p is None:
             return None
         self.p.terminate()
         self.p.wait()
-        self.f.flush()
-        rows = [l.strip().split(", ") for l in open(self.f.name) if l.strip()]
+        rows = self._rows()
         os.unlink(self.f.name)
+        # samples taken during the region; the last one before it when the region was
+        # shorter than the 200 ms sampling period
+        rows = rows[self.n0:] or rows[-1:]
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
@@ -530,6 +549,149 @@ def run_reference(args, rank, world):
 
 
 # --------------------------------------------------------------------- our arm
+def run_partition(args, rank, world, local):
+    """ONE fault (the workload) row-partitioned over the ranks, strong scaling: each
+    rank assembles and applies the operator of its tree-order rows and steps those
+    rows; per step one all-gather of the slip-rate deficit, and per attempt one
+    all-reduce (max) of the error maxima, with the step-size controller on the
+    device (PartitionedStepper.enqueue_device_step: no host read inside a step;
+    G steps captured in a CUDA graph, collectives included).  value = accepted
+    steps of the one fault / max over ranks of the timed region."""
+    import torch
+    import torch.distributed as dist
+    from pyquake3d_b200 import QDsim, read_mshV2
+    from pyquake3d_b200 import partition as P
+    dev = "cuda:%d" % local
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    msh, para = make_case(rank)                 # the same fault on every rank (seeded mesh)
+    nodes, tris = read_mshV2(msh)
+    t0 = time.perf_counter()
+    sim = QDsim(tris, nodes, para, device=dev, precision=args.precision)
+    st = sim.tree_block.struct
+    t_host = time.perf_counter() - t0
+    b = P.row_partition(st, world)
+    be = P.DeviceRowBackend(sim, st, int(b[rank]), int(b[rank + 1]), precision=args.precision, device=dev)
+    torch.cuda.synchronize()
+    t_asm = max_over_ranks(time.perf_counter() - t0 - t_host)
+    comm = P.TorchComm(use_dist=world > 1)
+    ps = P.PartitionedStepper([be], comm, sim.RelTol, attempts=args.attempts)
+    plan = be.op.plan(args.precision)
+
+    # warm-up (device-controlled, one host read at the end), then the graph
+    ps.run_device(args.warmup, sim.htry, chunk=args.warmup)
+    G = 50
+    graph = ps.capture(G) if args.steps % G == 0 else None
+    ok = max_over_ranks(0.0 if graph is not None else 1.0) == 0.0
+    if not ok:
+        graph = None                       # every rank launches alike
+    torch.cuda.synchronize()
+    pc0 = be.pc.cpu().numpy()
+    if pc0[P.PC_HALT] != 0:
+        raise RuntimeError("partitioned step halted during capture warm-up")
+    clk = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    if graph is not None:
+        for _ in range(args.steps // G):
+            graph.replay()
+    else:
+        for _ in range(args.steps):
+            ps.enqueue_device_step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clk.stop()
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    pc1 = be.pc.cpu().numpy()
+    done = int(pc1[P.PC_STEPS] - pc0[P.PC_STEPS])
+    halted = bool(pc1[P.PC_HALT] != 0)
+    if pc1[P.PC_STATUS] != 0:
+        raise RuntimeError("time step failed in the partitioned run")
+    if halted:
+        # the halted step and the rest of the timed count, outside the timed region
+        ps.time, ps.steps, ps.rejects = float(pc1[P.PC_TIME]), int(pc1[P.PC_STEPS]), int(pc1[P.PC_REJ])
+        h, dtnext = ps._attempts(float(pc1[P.PC_H]), int(pc1[P.PC_NRJCT]), False)
+        be.pc_resume(ps, dtnext, h)
+    del graph                              # holds NCCL calls: released before the group
+
+    # this rank's H-matvec alone (its rows' blocks), CUDA events
+    for _ in range(5):
+        be.op.matvec(be.xg_buf, args.precision, slots_only=True)
+    torch.cuda.synchronize()
+    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0.record()
+    for _ in range(50):
+        be.op.matvec(be.xg_buf, args.precision, slots_only=True)
+    m1.record()
+    torch.cuda.synchronize()
+    t_mv_rank = m0.elapsed_time(m1) / 1e3 / 50
+    t_mv = max_over_ranks(t_mv_rank)
+    bytes_all = float(plan["alg_bytes"])
+    if world > 1:
+        bt = torch.tensor([bytes_all], dtype=torch.float64, device=dev)
+        dist.all_reduce(bt)
+        bytes_all = float(bt.item())
+    hbm, peak_kind = peaks()
+
+    # end to end: the host reads the control block after every step (h, time, counters)
+    ne = min(args.steps, 100)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    hs = ps.run_device(ne, float(be.pc[P.PC_H]), chunk=1)
+    e1.record()
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    nl = (2 if plan["n_utasks"] > 0 or args.precision == "mixed" else 1) + 2 * args.attempts + 2
+    rows = int(b[rank + 1] - b[rank])
+    line = {
+        "metric": METRIC, "value": done / t, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t / max(done, 1), "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None,
+        "dtype": {"fp32": "f32 operator, f64 state", "bf16": "bf16+f32 operator, f64 state", "fp64": "f64",
+                  "mixed": "f32+f16+i8 operator, f32 accumulation, f64 state"}[args.precision],
+        "data": "synthetic",
+        "config": {"workload": CASE + " (%d triangles), one fault" % sim.xg.shape[0],
+                   "parallelism": "row partition x%d" % world, "precision": args.precision,
+                   "rows_per_rank": [int(b[r + 1] - b[r]) for r in range(world)],
+                   "attempt_slots": args.attempts, "cuda_graph_steps": G if ok and args.steps % G == 0 else 0,
+                   "l2": "inputs larger than L2 (operator %.2f GB per step over all ranks)" % (bytes_all / 1e9),
+                   "host_setup_s": round(t_host, 2), "assembly_s": round(t_asm, 2)},
+        "steps_done": done, "halted": halted,
+        "roofline": {"bound": "hbm", "achieved": bytes_all / t_mv / 1e9, "peak": hbm * world, "unit": "GB/s",
+                     "frac": bytes_all / t_mv / 1e9 / (hbm * world), "traffic": None,
+                     "kernel": "H-matvec of every rank's rows (slowest rank's time), %d GPUs" % world,
+                     "alg_bytes": bytes_all, "ms": 1e3 * t_mv, "peak_source": peak_kind},
+        "step_overhead_ms": 1e3 * (t / max(done, 1) - t_mv),
+        "e2e": {"value": ne / t_e2e, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 128,
+                "steps": ne, "path": "PartitionedStepper.run_device(chunk=1): the control block to the host "
+                                     "after every step (its accepted h)"},
+        "cpu_baseline": None,
+        "gpu_launches": nl * done,
+        "clocks": clocks,
+        "rank0_rows": rows, "rank0_matvec_ms": 1e3 * t_mv_rank, "e2e_last_h": hs[-1] if hs else None,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -548,6 +710,10 @@ def main():
                     help="horizon of the error study against the FP64 path (dt replay)")
     ap.add_argument("--precision", default="mixed", choices=["fp32", "bf16", "fp64", "mixed"],
                     help="operator storage of the headline path (mixed and fp32 meet the 1e-5 slip target)")
+    ap.add_argument("--parallelism", default="auto", choices=["auto", "partition", "replicas"],
+                    help="several GPUs: partition = one fault row-partitioned over the ranks (strong scaling, "
+                         "the default for N > 1); replicas = one fault per rank")
+    ap.add_argument("--attempts", type=int, default=3, help="attempt slots per partitioned step")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     set_case(args.case)
@@ -568,6 +734,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     torch.cuda.set_device(local)
+    if args.parallelism == "partition" or (args.parallelism == "auto" and world > 1):
+        run_partition(args, rank, world, local)
+        return
 
     # batched ensemble of 32 independent faults (one launch per step for all); run first,
     # on an empty device: its ACA workspaces (all live until packing) are the run's peak
@@ -786,7 +955,7 @@ def main():
                    "leaf": int(sim.tree_block.mini_leaf), "eta": 2.0, "aca": "relative 1e-5",
                    "mean_rank": float(np.mean(np.concatenate([kS, kD]))), "max_rank": int(max(kS.max(), kD.max())),
                    "l2": "inputs larger than L2 (operator %.2f GB per step)" % (plans[head]["alg_bytes"] / 1e9),
-                   "parallelism": "replicas x%d" % world, "host_setup_s": round(t_host, 2),
+                   "parallelism": "replicas x%d" % world if world > 1 else "single GPU", "host_setup_s": round(t_host, 2),
                    "assembly_s": round(t_asm, 2), "assembly_breakdown": {k: round(v, 3) for k, v in op.timings.items()}},
         "roofline": {"bound": "hbm", "achieved": mv[head]["GBs"], "peak": hbm, "unit": "GB/s",
                      "frac": mv[head]["frac"], "traffic": traffic,

@@ -169,6 +169,9 @@ size_t pq3d_item_bytes(int kind);
 int pq3d_hmatvec(const void *plan_host, const void *d_x, void *d_slots, void *d_tpart,
                  const double *d_add0, const double *d_add1,
                  const double *d_add2, double *d_y, cudaStream_t stream);
+/* Resident CTAs of the bulk-copy (streamed) mixed-storage kernel on the current
+ * device: the persistent grid its task lists are balanced for. */
+int pq3d_stream_ctas(void);
 
 /* ---------------------------------------------------------------- stepper */
 
@@ -198,6 +201,24 @@ int pq3d_rk_step(const void *args, int grid, cudaStream_t stream);
 int pq3d_rk_rows_attempt(const void *args, int grid, int r0, int r1, double h, int first, double *d_out,
                          cudaStream_t stream);
 int pq3d_rk_rows_accept(const void *args, int grid, int r0, int r1, double h, double *d_out, cudaStream_t stream);
+/* The same step with the controller on the device (the controller of
+ * src/QDsim.py:931-958, as the host form applies it): every rank keeps a control
+ * block pc (16 doubles: [0] h of the next attempt, [1] dtnext, [2] time, [3]
+ * rejects this step, [4] status, [5] accepted, [6] max|V1|, [7] max|V2|, [8]
+ * steps, [9] total rejects, [10] halt, [11] first attempt pending, [12] attempts
+ * this step) and receives the same maxima reduced over ranks, so all ranks decide
+ * alike without the host.  A step is the fixed sequence attempt_dev -> reduce ->
+ * control (max_attempts times), accept_dev -> reduce -> finish; kernels skip
+ * their work once the step is accepted or halted.  control halts with status 0
+ * after max_attempts rejected attempts (the host then finishes the step) and with
+ * PQ3D_ERR_DT when the step is given up; finish prepares the next step
+ * (h = dtnext, counters). */
+int pq3d_rk_rows_attempt_dev(const void *args, int grid, int r0, int r1, const double *d_pc, double *d_out,
+                             cudaStream_t stream);
+int pq3d_rk_rows_control(double *d_pc, const double *d_E8, double reltol, int max_attempts, cudaStream_t stream);
+int pq3d_rk_rows_accept_dev(const void *args, int grid, int r0, int r1, const double *d_pc, double *d_out,
+                            cudaStream_t stream);
+int pq3d_rk_rows_finish(double *d_pc, const double *d_V8, cudaStream_t stream);
 
 /* ---------------------------------------------------------------- ensemble
  * Many independent faults stepped together (the reference runs one fault per

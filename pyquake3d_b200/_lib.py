@@ -126,6 +126,10 @@ def load():
     L.pq3d_rk_step.argtypes = [vp, i32, vp]
     L.pq3d_rk_rows_attempt.argtypes = [vp, i32, i32, i32, ctypes.c_double, i32, vp, vp]
     L.pq3d_rk_rows_accept.argtypes = [vp, i32, i32, i32, ctypes.c_double, vp, vp]
+    L.pq3d_rk_rows_attempt_dev.argtypes = [vp, i32, i32, i32, vp, vp, vp]
+    L.pq3d_rk_rows_control.argtypes = [vp, vp, ctypes.c_double, i32, vp]
+    L.pq3d_rk_rows_accept_dev.argtypes = [vp, i32, i32, i32, vp, vp, vp]
+    L.pq3d_rk_rows_finish.argtypes = [vp, vp, vp]
     L.pq3d_host_map_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(vp), ctypes.POINTER(vp)]
     L.pq3d_host_map_free.argtypes = [vp]
     L.pq3d_event_create.argtypes = [ctypes.POINTER(vp)]
@@ -141,6 +145,7 @@ def load():
               "pq3d_aca_batched", "pq3d_aca_pack", "pq3d_hmatvec", "pq3d_nearfield_rowabs", "pq3d_aca_term_weights",
               "pq3d_aca_pack_mixed", "pq3d_rk_grid", "pq3d_rk_step", "pq3d_ens_grid",
               "pq3d_ens_step", "pq3d_ens_task_rows", "pq3d_rk_rows_attempt", "pq3d_rk_rows_accept",
+              "pq3d_rk_rows_attempt_dev", "pq3d_rk_rows_control", "pq3d_rk_rows_accept_dev", "pq3d_rk_rows_finish",
               "pq3d_host_map_alloc", "pq3d_host_map_free", "pq3d_event_create", "pq3d_event_destroy",
               "pq3d_event_record", "pq3d_event_sync", "pq3d_event_query", "pq3d_snapshot", "pq3d_stream_wait_event"):
         getattr(L, f).restype = ctypes.c_int

@@ -308,6 +308,108 @@ __global__ void __launch_bounds__(RK_THREADS) k_rk_rows_accept(RkArgs A, int r0,
     rows_finish<RK_THREADS>(A, v4, out);
 }
 
+// ---------------------------------------------------------------------------
+// Row-partitioned step with the controller on the device.  Every rank keeps the
+// same control block pc (PC_* below) and applies the same controller to the same
+// maxima reduced over ranks, so all ranks take identical decisions without the
+// host: a step is a fixed launch sequence (gather, matvec, R x [attempt, reduce,
+// control], accept, reduce, finish) that can be enqueued or captured ahead.  An
+// attempt after acceptance, or anything after a halt, returns at once.  A step
+// that needs more than R attempts halts (status 0): the host finishes it.
+enum {
+    PC_H = 0,        // trial size of the next attempt
+    PC_DTNEXT = 1,   // the controller's next size
+    PC_TIME = 2,
+    PC_NRJCT = 3,    // rejections in this step
+    PC_STATUS = 4,   // PQ3D_ERR_DT when the step was given up
+    PC_ACC = 5,      // this step's attempt was accepted
+    PC_V1 = 6, PC_V2 = 7,   // max |V1|, max |V2| after the last accepted step
+    PC_STEPS = 8, PC_REJ = 9,
+    PC_HALT = 10,    // no further work until the host resumes
+    PC_FIRST = 11,   // the next attempt is the step's first (sums the matvec slots)
+    PC_ATT = 12      // attempts in this step
+};
+
+__global__ void __launch_bounds__(RK_THREADS) k_rk_rows_attempt_dev(RkArgs A, int r0, int r1, const double *pc,
+                                                                    double *out)
+{
+    if (pc[PC_HALT] != 0.0 || pc[PC_ACC] != 0.0) return;     // the same for every CTA
+    const double h = pc[PC_H];
+    const bool first = pc[PC_FIRST] != 0.0;
+    double e4[4] = {0.0, 0.0, 0.0, 0.0};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    if (first && A.fuse_rowsum)
+        for (int64_t base = r0 + (int64_t)blockIdx.x * RK_THREADS; base < r1; base += stride)
+            rowsum_cta<RK_THREADS>(A, base, r1);
+    for (int64_t i = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < r1; i += stride) {
+        double e[4];
+        dp54_element(A, i, h, e);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) e4[q] = nanmax(e4[q], e[q]);
+    }
+    rows_finish<RK_THREADS>(A, e4, out);
+}
+
+// The reference's controller on the reduced maxima E8 (values with NaN -> 0, then
+// NaN flags), one thread.
+__global__ void k_rk_rows_control(double *pc, const double *E8, double reltol, int max_attempts)
+{
+    if (pc[PC_HALT] != 0.0 || pc[PC_ACC] != 0.0) return;
+    double E[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) E[q] = E8[4 + q] > 0.0 ? __longlong_as_double(0x7ff8000000000000ll) : E8[q];
+    StepCtl c{pc[PC_H], 0.0, (int)pc[PC_NRJCT], (int)pc[PC_ATT], false};
+    const bool done = controller(c, E, reltol, false);
+    pc[PC_ATT] = c.attempt;
+    pc[PC_FIRST] = 0.0;
+    pc[PC_DTNEXT] = c.dtnext;
+    if (c.accepted) {
+        pc[PC_ACC] = 1.0;
+        return;
+    }
+    pc[PC_NRJCT] = c.nrjct;
+    pc[PC_H] = c.h;
+    if (done) {
+        pc[PC_STATUS] = (double)PQ3D_ERR_DT;
+        pc[PC_HALT] = 1.0;
+    } else if (c.attempt >= max_attempts) {
+        pc[PC_HALT] = 1.0;                 // more attempts than launched: the host continues
+    }
+}
+
+__global__ void __launch_bounds__(RK_THREADS) k_rk_rows_accept_dev(RkArgs A, int r0, int r1, const double *pc,
+                                                                   double *out)
+{
+    if (pc[PC_HALT] != 0.0 || pc[PC_ACC] == 0.0) return;
+    const double h = pc[PC_H];
+    double v4[4] = {0.0, 0.0, 0.0, 0.0};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < r1; i += stride) {
+        double v1, v2;
+        accept_element(A, i, h, v1, v2);
+        v4[0] = fmax(v4[0], fabs(v1));
+        v4[1] = fmax(v4[1], fabs(v2));
+    }
+    rows_finish<RK_THREADS>(A, v4, out);
+}
+
+// After the accepted step (maxima V8 reduced over ranks): time, counters, and the
+// next step's trial size.
+__global__ void k_rk_rows_finish(double *pc, const double *V8)
+{
+    if (pc[PC_HALT] != 0.0 || pc[PC_ACC] == 0.0) return;
+    pc[PC_TIME] += pc[PC_H];
+    pc[PC_STEPS] += 1.0;
+    pc[PC_REJ] += pc[PC_NRJCT];
+    pc[PC_V1] = V8[0];
+    pc[PC_V2] = V8[1];
+    pc[PC_H] = pc[PC_DTNEXT];
+    pc[PC_NRJCT] = 0.0;
+    pc[PC_ACC] = 0.0;
+    pc[PC_ATT] = 0.0;
+    pc[PC_FIRST] = 1.0;
+}
+
 }  // namespace
 
 PQ3D_EXPORT size_t pq3d_rk_args_bytes(void) { return sizeof(RkArgs); }
@@ -342,6 +444,45 @@ PQ3D_EXPORT int pq3d_rk_rows_attempt(const void *args, int grid, int r0, int r1,
     if (rc != PQ3D_OK) return rc;
     if (first && A.fuse_rowsum && (!A.slots || !A.leaf_of_row || !A.leaf_ptr || !A.leaf_off)) return PQ3D_ERR_ARG;
     k_rk_rows_attempt<<<grid, RK_THREADS, 0, stream>>>(A, r0, r1, h, first, d_out);
+    return pq3d_launch_status();
+}
+
+// Device-controlled forms (control block pc, 16 doubles, see PC_* in this file).
+PQ3D_EXPORT int pq3d_rk_rows_attempt_dev(const void *args, int grid, int r0, int r1, const double *d_pc,
+                                         double *d_out, cudaStream_t stream)
+{
+    if (!args || !d_pc) return PQ3D_ERR_ARG;
+    const RkArgs A = *(const RkArgs *)args;
+    const int rc = rows_check(A, grid, r0, r1, d_out);
+    if (rc != PQ3D_OK) return rc;
+    if (A.fuse_rowsum && (!A.slots || !A.leaf_of_row || !A.leaf_ptr || !A.leaf_off)) return PQ3D_ERR_ARG;
+    k_rk_rows_attempt_dev<<<grid, RK_THREADS, 0, stream>>>(A, r0, r1, d_pc, d_out);
+    return pq3d_launch_status();
+}
+
+PQ3D_EXPORT int pq3d_rk_rows_control(double *d_pc, const double *d_E8, double reltol, int max_attempts,
+                                     cudaStream_t stream)
+{
+    if (!d_pc || !d_E8 || max_attempts < 1 || !(reltol > 0.0)) return PQ3D_ERR_ARG;
+    k_rk_rows_control<<<1, 1, 0, stream>>>(d_pc, d_E8, reltol, max_attempts);
+    return pq3d_launch_status();
+}
+
+PQ3D_EXPORT int pq3d_rk_rows_accept_dev(const void *args, int grid, int r0, int r1, const double *d_pc,
+                                        double *d_out, cudaStream_t stream)
+{
+    if (!args || !d_pc) return PQ3D_ERR_ARG;
+    const RkArgs A = *(const RkArgs *)args;
+    const int rc = rows_check(A, grid, r0, r1, d_out);
+    if (rc != PQ3D_OK) return rc;
+    k_rk_rows_accept_dev<<<grid, RK_THREADS, 0, stream>>>(A, r0, r1, d_pc, d_out);
+    return pq3d_launch_status();
+}
+
+PQ3D_EXPORT int pq3d_rk_rows_finish(double *d_pc, const double *d_V8, cudaStream_t stream)
+{
+    if (!d_pc || !d_V8) return PQ3D_ERR_ARG;
+    k_rk_rows_finish<<<1, 1, 0, stream>>>(d_pc, d_V8);
     return pq3d_launch_status();
 }
 

@@ -31,7 +31,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import check, ptr
-from .hmatrix import ClusterNode, LeafBlock, DTYPES, _CW_LR, _cdiv
+from .hmatrix import ClusterNode, LeafBlock, DTYPES, MIXED_TOL, _CW_LR, _cdiv
 
 
 # ----------------------------------------------------------------------------- host partition
@@ -209,17 +209,34 @@ class TorchComm:
             out = [torch.zeros_like(n) for _ in range(self.dist.get_world_size())]
             self.dist.all_gather(out, n)
             sizes = self._sizes = [int(v.item()) for v in out]
+            self._gbuf = None
         m = max(sizes)
-        pad = t if t.numel() == m else torch.cat([t, t.new_zeros(m - t.numel())])
-        out = [torch.empty_like(pad) for _ in sizes]
-        self.dist.all_gather(out, pad.contiguous())
-        return torch.cat([o[:k] for o, k in zip(out, sizes)])
+        g = getattr(self, "_gbuf", None)
+        if g is None or g.dtype != t.dtype or g.device != t.device:
+            # one all-gather into a persistent buffer (world x longest piece); the pieces
+            # are then picked out by one index gather when their lengths differ
+            self._gbuf = torch.empty(len(sizes) * m, dtype=t.dtype, device=t.device)
+            self._gpad = torch.zeros(m, dtype=t.dtype, device=t.device)
+            idx = np.concatenate([np.arange(r * m, r * m + k) for r, k in enumerate(sizes)])
+            self._gidx = None if min(sizes) == m else torch.tensor(idx, dtype=torch.int64, device=t.device)
+        if t.numel() == m:
+            pad = t.contiguous()
+        else:
+            self._gpad[:t.numel()].copy_(t)
+            pad = self._gpad
+        self.dist.all_gather_into_tensor(self._gbuf, pad)
+        return self._gbuf if self._gidx is None else self._gbuf.index_select(0, self._gidx)
 
     def max(self, parts):
         t = self._local(parts, self.torch.maximum)
         if self.use_dist:
             self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return t
+
+
+# control block of the device-controlled step (pq3d_rk_rows_control, include/pq3d.h)
+PC_H, PC_DTNEXT, PC_TIME, PC_NRJCT, PC_STATUS, PC_ACC, PC_V1, PC_V2, PC_STEPS, PC_REJ, PC_HALT, PC_FIRST, PC_ATT = range(13)
+PC_LASTH = 13          # kept on the host side of the record: the last accepted h (written by pc_resume / finish)
 
 
 def _nan_encode(v):
@@ -258,10 +275,11 @@ class PartitionedStepper:
       accept(h)         accepted-step update of its rows -> (max|V1|, max|V2|, 0, 0 flags)
     comm: gather / max over all ranks (TorchComm)."""
 
-    def __init__(self, backends, comm, reltol):
+    def __init__(self, backends, comm, reltol, attempts=3):
         self.backends = list(backends)
         self.comm = comm
         self.reltol = float(reltol)
+        self.attempts = int(attempts)      # attempt slots per step of the device-controlled run
         self.time = 0.0
         self.steps = 0
         self.rejects = 0
@@ -271,9 +289,11 @@ class PartitionedStepper:
         xt = self.comm.gather([b.x_rows() for b in self.backends])
         for b in self.backends:
             b.matvec_gathered(xt)
-        h = float(dttry)
-        nrjct = 0
-        first = True
+        return self._attempts(float(dttry), 0, True, h_forced)
+
+    def _attempts(self, h, nrjct, first, h_forced=None):
+        """Attempts of one step from trial size h (nrjct rejections so far) until one is
+        accepted, then the accepted update; returns (h, dtnext)."""
         while True:
             if h_forced is not None:
                 h = float(h_forced)
@@ -298,6 +318,82 @@ class PartitionedStepper:
         self.steps += 1
         self.rejects += nrjct
         return h, dtnext
+
+    # ------------------------------------------------------------------ controller on the device
+    def enqueue_device_step(self):
+        """One step as a fixed launch sequence with the controller on the device: the
+        deficit gather and the matvec, then `attempts` x (attempt, max over ranks,
+        controller), then the accepted update, max over ranks, finish.  No host
+        synchronisation: steps can be enqueued back to back (or captured).  Every
+        rank issues the same collectives in the same order whatever the decisions."""
+        xt = self.comm.gather([b.x_rows() for b in self.backends])
+        for b in self.backends:
+            b.matvec_gathered(xt)
+        for _ in range(self.attempts):
+            E = self.comm.max([b.attempt_dev() for b in self.backends])
+            for b in self.backends:
+                b.control(E, self.reltol, self.attempts)
+        V = self.comm.max([b.accept_dev() for b in self.backends])
+        for b in self.backends:
+            b.finish(V)
+
+    def run_device(self, nsteps, dttry, chunk=None):
+        """nsteps steps with the controller on the device, enqueued `chunk` at a time
+        (default: all); the host reads the control block once per chunk.  A step that
+        needs more attempts than the launched slots halts the device sequence and is
+        finished here with the host controller (same decisions), after which the
+        device run resumes.  Returns the accepted step sizes when chunk == 1, else the
+        last one's (h, dtnext)."""
+        for b in self.backends:
+            b.pc_start(dttry, self)
+        chunk = int(chunk or nsteps)
+        hs = []
+        done = 0
+        while done < nsteps:
+            k = min(chunk, nsteps - done)
+            s0 = self.steps
+            for _ in range(k):
+                self.enqueue_device_step()
+            pc = self.backends[0].pc.cpu().numpy()
+            ran = int(pc[PC_STEPS]) - s0
+            self.steps, self.time = int(pc[PC_STEPS]), float(pc[PC_TIME])
+            self.rejects, self.vmax = int(pc[PC_REJ]), (float(pc[PC_V1]), float(pc[PC_V2]))
+            if chunk == 1 and ran == 1:
+                hs.append(float(self.last_h()))
+            done += ran
+            if pc[PC_HALT] != 0.0:
+                if pc[PC_STATUS] != 0.0:
+                    raise _lib.Pq3dError("time step failed: h < 1e-15 or more than 20 rejections")
+                # the halted step: the host's attempts from where the device stopped
+                h, dtnext = self._attempts(float(pc[PC_H]), int(pc[PC_NRJCT]), False)
+                hs.append(h) if chunk == 1 else None
+                done += 1
+                for b in self.backends:
+                    b.pc_resume(self, dtnext, h)
+        return hs if chunk == 1 else (self.last_h(), float(self.backends[0].pc[PC_H]))
+
+    def last_h(self):
+        return float(self.backends[0].pc[PC_LASTH])
+
+    def capture(self, nsteps):
+        """CUDA graph of nsteps device-controlled steps (enqueue_device_step); replays
+        chain on the control blocks.  The communicator's collectives are captured
+        with the kernels, so every rank must capture and replay alike.  Returns None
+        when capture is not possible here."""
+        import torch
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        try:
+            with torch.cuda.stream(s):
+                with torch.cuda.graph(g, stream=s):
+                    for _ in range(nsteps):
+                        self.enqueue_device_step()
+        except (RuntimeError, _lib.Pq3dError):
+            torch.cuda.synchronize()
+            return None
+        torch.cuda.current_stream().wait_stream(s)
+        return g
 
 
 # ----------------------------------------------------------------------------- device backend
@@ -327,7 +423,8 @@ class DeviceRowBackend:
             from .qdsim import hs_mode
             op = DeviceHMatrix(self.rs, sim.xg, sim.eleVec, sim.nodelst, sim.elelst, sim.mu, sim.lambda_,
                                device=device, aca_tol=float(P.get("ACA tolerance", 0.01)),
-                               aca_rel=P.get("ACA relative tolerance", "False") == "True", halfspace=hs_mode(sim))
+                               aca_rel=P.get("ACA relative tolerance", "False") == "True", halfspace=hs_mode(sim),
+                               mixed_tol=float(P.get("Mixed precision tolerance", MIXED_TOL)))
             op.assemble(("fp64",) if precision == "fp64" else ("fp64", precision))
         self.op = op
         n = self.n = struct.n
@@ -412,3 +509,46 @@ class DeviceRowBackend:
     def get(self, name):
         """This rank's rows of a state vector (tree order slice [r0, r1))."""
         return self.t[name][self.r0:self.r1].cpu().numpy()
+
+    # ------------------------------------------------------------------ controller on the device
+    def pc_start(self, dttry, ps):
+        """Control block for a device-controlled run from trial size dttry."""
+        pc = np.zeros(16)
+        pc[PC_H], pc[PC_TIME], pc[PC_STEPS], pc[PC_REJ] = dttry, ps.time, ps.steps, ps.rejects
+        pc[PC_V1], pc[PC_V2] = ps.vmax
+        pc[PC_FIRST] = 1.0
+        if getattr(self, "pc", None) is None:
+            self.pc = self.torch.tensor(pc, dtype=self.torch.float64, device=self.op.dev)
+            self.E8 = self.torch.zeros(8, dtype=self.torch.float64, device=self.op.dev)
+        else:
+            self.pc.copy_(self.torch.tensor(pc, dtype=self.torch.float64))   # captured graphs keep the address
+
+    def pc_resume(self, ps, dtnext, h):
+        """After the host finished a halted step: the next step from dtnext."""
+        pc = np.zeros(16)
+        pc[PC_H], pc[PC_TIME], pc[PC_STEPS], pc[PC_REJ] = dtnext, ps.time, ps.steps, ps.rejects
+        pc[PC_V1], pc[PC_V2] = ps.vmax
+        pc[PC_FIRST], pc[PC_LASTH] = 1.0, h
+        self.pc.copy_(self.torch.tensor(pc, dtype=self.torch.float64))
+
+    def attempt_dev(self):
+        check(self.L.pq3d_rk_rows_attempt_dev(self.args.ctypes.data, self.grid, self.r0, self.r1, ptr(self.pc),
+                                              ptr(self.out), _lib.stream_ptr()), "pq3d_rk_rows_attempt_dev")
+        return self.out
+
+    def control(self, E, reltol, attempts):
+        # the reduced maxima may live in a buffer the next reduction reuses: keep a copy
+        self.E8.copy_(E)
+        check(self.L.pq3d_rk_rows_control(ptr(self.pc), ptr(self.E8), float(reltol), int(attempts),
+                                          _lib.stream_ptr()), "pq3d_rk_rows_control")
+
+    def accept_dev(self):
+        # the accepted h, for the host record, before finish replaces pc[PC_H] by dtnext
+        self.pc[PC_LASTH:PC_LASTH + 1].copy_(self.pc[PC_H:PC_H + 1])
+        check(self.L.pq3d_rk_rows_accept_dev(self.args.ctypes.data, self.grid, self.r0, self.r1, ptr(self.pc),
+                                             ptr(self.out), _lib.stream_ptr()), "pq3d_rk_rows_accept_dev")
+        return self.out
+
+    def finish(self, V):
+        self.E8.copy_(V)
+        check(self.L.pq3d_rk_rows_finish(ptr(self.pc), ptr(self.E8), _lib.stream_ptr()), "pq3d_rk_rows_finish")

@@ -67,6 +67,93 @@ class NumpyRowBackend:
         st.slip2[r] = st.slip2[r] + v2 * h
         return torch.tensor([np.max(np.abs(v1)), np.max(np.abs(v2)), 0, 0, 0, 0, 0, 0], dtype=torch.float64)
 
+    # The device-controlled forms: the kernels of pq3d_rk_rows_attempt_dev / control /
+    # accept_dev / finish (pyquake3d_b200/csrc/rk.cu) emulated on a CPU control block,
+    # so that PartitionedStepper.run_device runs over gloo.
+    def _pc(self, ps, h, lasth=0.0):
+        from pyquake3d_b200 import partition as P
+        pc = np.zeros(16)
+        pc[P.PC_H], pc[P.PC_TIME], pc[P.PC_STEPS], pc[P.PC_REJ] = h, ps.time, ps.steps, ps.rejects
+        pc[P.PC_V1], pc[P.PC_V2] = ps.vmax
+        pc[P.PC_FIRST], pc[P.PC_LASTH] = 1.0, lasth
+        return torch.tensor(pc)
+
+    def pc_start(self, dttry, ps):
+        self.pc = self._pc(ps, dttry)
+        self.out = torch.zeros(8, dtype=torch.float64)
+
+    def pc_resume(self, ps, dtnext, h):
+        self.pc = self._pc(ps, dtnext, h)
+
+    def attempt_dev(self):
+        from pyquake3d_b200 import partition as P
+        pc = self.pc
+        if pc[P.PC_HALT] == 0 and pc[P.PC_ACC] == 0:
+            self.out = self.attempt(float(pc[P.PC_H]), pc[P.PC_FIRST] != 0)
+        return self.out
+
+    def control(self, E8, reltol, attempts):
+        from pyquake3d_b200 import partition as P
+        pc = self.pc
+        if pc[P.PC_HALT] != 0 or pc[P.PC_ACC] != 0:
+            return
+        E = np.where(E8[4:].numpy() > 0, np.nan, E8[:4].numpy())
+        mx, mn = P._py_max, P._py_min             # the comparison forms of the kernels (NaN order)
+        h = float(pc[P.PC_H])
+        R1, R2 = E[0] + 1e-10, mx(mx(E[1], E[2]), E[3]) + 1e-10
+        c1, c2 = R1 / reltol, R2 / reltol
+        hn1, hn2 = h * 0.9 * (reltol / R1) ** 0.2, h * 0.9 * (reltol / R2) ** 0.2
+        pc[P.PC_ATT] += 1
+        pc[P.PC_FIRST] = 0
+        if mx(c1, c2) < 1.0 and not (np.isnan(c1) or np.isnan(c2)):
+            pc[P.PC_DTNEXT] = mn(mn(hn1, hn2), 1.5 * h)
+            pc[P.PC_ACC] = 1
+            return
+        pc[P.PC_DTNEXT] = mn(hn1, hn2)
+        pc[P.PC_NRJCT] += 1
+        pc[P.PC_H] = mx(0.5 * h, float(pc[P.PC_DTNEXT]))
+        if pc[P.PC_H] < 1e-15 or pc[P.PC_NRJCT] > 20:
+            pc[P.PC_STATUS], pc[P.PC_HALT] = 1, 1
+        elif pc[P.PC_ATT] >= attempts:
+            pc[P.PC_HALT] = 1
+
+    def accept_dev(self):
+        from pyquake3d_b200 import partition as P
+        pc = self.pc
+        pc[P.PC_LASTH] = pc[P.PC_H]
+        if pc[P.PC_HALT] == 0 and pc[P.PC_ACC] != 0:
+            self.out = self.accept(float(pc[P.PC_H]))
+        return self.out
+
+    def finish(self, V8):
+        from pyquake3d_b200 import partition as P
+        pc = self.pc
+        if pc[P.PC_HALT] != 0 or pc[P.PC_ACC] == 0:
+            return
+        pc[P.PC_TIME] += pc[P.PC_H]
+        pc[P.PC_STEPS] += 1
+        pc[P.PC_REJ] += pc[P.PC_NRJCT]
+        pc[P.PC_V1], pc[P.PC_V2] = V8[0], V8[1]
+        pc[P.PC_H] = pc[P.PC_DTNEXT]
+        pc[P.PC_NRJCT] = pc[P.PC_ACC] = pc[P.PC_ATT] = 0
+        pc[P.PC_FIRST] = 1
+
+
+def run_rank_device(rank, world, files, steps, dttry_scale, attempts, seed=7):
+    """run_device over gloo from a trial size dttry_scale x the initial one;
+    returns (accepted sizes, rejections)."""
+    from pyquake3d_b200 import QDsim, read_mshV2
+    from pyquake3d_b200.partition import PartitionedStepper, RankStructure, TorchComm, row_partition
+    msh, para = files
+    nodes, tris = read_mshV2(msh)
+    sim = QDsim(tris, nodes, para)
+    st = sim.tree_block.struct
+    b = row_partition(st, world)
+    rs = RankStructure(st, b[rank], b[rank + 1], seed=seed)
+    ps = PartitionedStepper([NumpyRowBackend(sim, rs)], TorchComm(use_dist=True), sim.RelTol, attempts=attempts)
+    hs = ps.run_device(steps, sim.htry * dttry_scale, chunk=1)
+    return np.array(hs), ps.rejects
+
 
 def run_rank(rank, world, files, steps=30, seed=7):
     from pyquake3d_b200 import QDsim, read_mshV2

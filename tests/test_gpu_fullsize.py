@@ -174,6 +174,45 @@ def test_two_ranks_follow_fused_step_thrust20k(lib, tmp_path_factory):
         assert np.abs(got - want).max() <= 1e-9 * np.abs(want).max(), k
 
 
+def test_two_ranks_device_controller_graph_thrust20k(lib, tmp_path_factory):
+    """The row partition with the controller on the device, 20 steps as two
+    replays of a captured 10-step graph (collectives and control kernels
+    included), mixed storage, two ranks emulated in one process: the fused
+    single-GPU mixed step's sizes and states (the ranks' operators hold the same
+    term classes; their FP32 sums run in another order)."""
+    from pyquake3d_b200 import partition as P
+    from pyquake3d_b200.qdsim import DeviceStepper
+    sim = _case("thrust20k", tmp_path_factory, "mixed")
+    op = sim.tree_block.op()
+    st = sim.tree_block.struct
+    ref = DeviceStepper(sim, op, "mixed")
+    h_ref = ref.run(21, sim.htry)[:, 0]
+    b = P.row_partition(st, 2)
+    backends = [P.DeviceRowBackend(sim, st, b[r], b[r + 1], precision="mixed") for r in range(2)]
+    ps = P.PartitionedStepper(backends, P.TorchComm(use_dist=False), sim.RelTol, attempts=3)
+    h1 = ps.run_device(1, sim.htry, chunk=1)
+    g = ps.capture(10)
+    assert g is not None
+    torch.cuda.synchronize()
+    hs = list(h1)
+    for _ in range(2):
+        s0 = int(backends[0].pc[P.PC_STEPS].item())
+        g.replay()
+        torch.cuda.synchronize()
+        pc = backends[0].pc.cpu().numpy()
+        assert pc[P.PC_HALT] == 0 and pc[P.PC_STATUS] == 0
+        assert int(pc[P.PC_STEPS]) - s0 == 10
+        hs.append(float(pc[P.PC_LASTH]))
+    np.testing.assert_allclose(hs, h_ref[[0, 10, 20]], rtol=1e-6)
+    for be in backends:
+        np.testing.assert_array_equal(be.pc.cpu().numpy()[:13], backends[0].pc.cpu().numpy()[:13])
+    np.testing.assert_allclose(float(backends[0].pc[P.PC_TIME]), h_ref.sum(), rtol=1e-6)
+    for k in ("slip", "psi", "Tt"):
+        got = np.concatenate([be.get(k) for be in backends])
+        want = ref.t[k].cpu().numpy()
+        assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max(), k
+
+
 def test_plain2k_device_follows_oracle_on_same_operator(lib, tmp_path_factory):
     """plain2k at full size (1,936 triangles, one dense FP64 block): sampled rows
     of the device-assembled operator equal the C oracle's Green's function to

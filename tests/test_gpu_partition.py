@@ -5,7 +5,10 @@ step kernels); the ranks of one process are reduced by TorchComm on the host
 side of plain launches, so no kernel waits for another.  Two ranks follow the
 reference's 30-step dt sequence of the tiny case (FP64 operator, 1e-8 as the
 single-GPU stepper), and three ranks (low-rank blocks shared across cuts) follow
-the fused single-GPU step on the FP32 operator."""
+the fused single-GPU step on the FP32 operator.  With the controller on the
+device (pq3d_rk_rows_control) the two ranks take the same decisions without a
+host read per attempt, and a step that outruns the attempt slots is finished by
+the host controller exactly as the host-controlled run takes it."""
 import numpy as np
 import pytest
 
@@ -67,3 +70,62 @@ def test_three_ranks_with_shared_blocks_follow_fused_step(lib, tiny_files, tiny_
     slip = np.concatenate([be.get("slip1") for be in backends])
     ref = st.t["slip1"].cpu().numpy()
     assert np.abs(slip - ref).max() <= 1e-9 * np.abs(ref).max()
+
+
+def _backends(sim, R, precision, slack=0.02):
+    from pyquake3d_b200.partition import DeviceRowBackend, row_partition
+    st = sim.tree_block.struct
+    b = row_partition(st, R, slack=slack)
+    return [DeviceRowBackend(sim, st, b[r], b[r + 1], precision=precision) for r in range(R)]
+
+
+@pytest.mark.parametrize("chunk", [1, 10])
+def test_device_controller_follows_reference(lib, tiny_files, tiny_golden, chunk):
+    """The controller on the device (a fixed launch sequence per step, the host
+    reading the control block once per chunk) takes the reference's decisions."""
+    from pyquake3d_b200.partition import PartitionedStepper, TorchComm
+    g = tiny_golden
+    sim = _sim(tiny_files, int(g["aca_seed"]))
+    backends = _backends(sim, 2, "fp64")
+    ps = PartitionedStepper(backends, TorchComm(use_dist=False), sim.RelTol, attempts=3)
+    out = ps.run_device(30, sim.htry, chunk=chunk)
+    if chunk == 1:
+        np.testing.assert_allclose(out, g["steps_h"], rtol=1e-8)
+    else:
+        np.testing.assert_allclose(out[0], g["steps_h"][-1], rtol=1e-8)
+    assert ps.steps == 30
+    np.testing.assert_allclose(ps.time, np.sum(g["steps_h"]), rtol=1e-8)
+    slip = np.concatenate([be.get("slip") for be in backends])
+    ref = g["step30_slip"][sim.tree_block.struct.perm]
+    assert np.abs(slip - ref).max() <= 1e-7 * np.abs(ref).max()
+    assert all(be.pc[4].item() == 0.0 and be.pc[10].item() == 0.0 for be in backends)
+
+
+@pytest.mark.parametrize("attempts,k", [(1, 36), (3, 40)])
+def test_device_controller_halts_and_host_finishes(lib, tiny_files, tiny_golden, attempts, k):
+    """A first trial size of 2^k times the initial one (about 2 and 35 years; the
+    oracle rejects it 5 and 9 times, NaN attempts among the latter): the first step
+    outruns the attempt slots, the device halts it, the host finishes it with the
+    same controller and the device run resumes; steps, rejections, sizes and state
+    equal the host-controlled run from the same trial size."""
+    from pyquake3d_b200.partition import PartitionedStepper, TorchComm
+    seed = int(tiny_golden["aca_seed"])
+    sim_a = _sim(tiny_files, seed)
+    sim_b = _sim(tiny_files, seed)
+    dttry = sim_a.htry * 2.0 ** k
+    ba = _backends(sim_a, 2, "fp64")
+    pa = PartitionedStepper(ba, TorchComm(use_dist=False), sim_a.RelTol, attempts=attempts)
+    ha = pa.run_device(12, dttry, chunk=1)
+    bb = _backends(sim_b, 2, "fp64")
+    pb = PartitionedStepper(bb, TorchComm(use_dist=False), sim_b.RelTol)
+    hb = []
+    dt = dttry
+    for _ in range(12):
+        h, dt = pb.step(dt)
+        hb.append(h)
+    assert pb.rejects > attempts                 # the first step did outrun the slots
+    np.testing.assert_allclose(ha, hb, rtol=1e-12)
+    assert (pa.steps, pa.rejects) == (pb.steps, pb.rejects)
+    for x, y in zip(ba, bb):
+        np.testing.assert_allclose(x.get("slip1"), y.get("slip1"), rtol=1e-12, atol=1e-300)
+        np.testing.assert_allclose(x.get("psi"), y.get("psi"), rtol=1e-12)

@@ -128,6 +128,61 @@ def test_two_gloo_ranks_follow_reference(tiny_files, tiny_golden):
     assert np.array_equal(res[0], res[1])
 
 
+def _worker_device(rank, world, port, files, out_q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        from partition_numpy_backend import run_rank_device
+        out_q.put((rank, run_rank_device(rank, world, files, 8, 2.0 ** 36, attempts=1)))
+    except Exception as e:
+        out_q.put((rank, repr(e)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_device_controller(tiny_files, tiny_golden):
+    """PartitionedStepper.run_device over two gloo ranks, the control kernels
+    emulated on the CPU, one attempt slot per step and a first trial size 2^36
+    times the initial one: the first step is rejected 5 times, so the device
+    sequence halts and the host controller finishes it; every rank issues the
+    same collectives whatever the decisions.  Sizes and rejections equal the
+    oracle's single-process stepping from the same trial size."""
+    import torch.multiprocessing as mp
+    import qd_oracle
+    from pyquake3d_b200 import QDsim, read_mshV2
+    nodes, tris = read_mshV2(tiny_files[0])
+    sim = QDsim(tris, nodes, tiny_files[1])
+    st = sim.tree_block.struct
+    geo = qd_oracle.Geometry(sim.xg, sim.eleVec, sim.nodelst, sim.elelst, sim.mu, sim.lambda_)
+    op = qd_oracle.OracleOperator(geo, [(b.row.indices, b.col.indices, b.aca) for b in st.blocks],
+                                  aca_start_indices(st.blocks, 7), eps=0.01)
+    ref = qd_oracle.OracleStepper(qd_oracle.sim_state(sim), qd_oracle.operator_mvm(op), sim.V0, sim.mu, sim.Cs,
+                                  sim.RelTol, sim.fix_Tn)
+    dt, hs, rej = sim.htry * 2.0 ** 36, [], 0
+    for _ in range(8):
+        h, dt = ref.simu_forward(dt)
+        hs.append(h)
+        rej += ref.nrjct
+    assert rej >= 5
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker_device, args=(r, 2, port, tiny_files, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=600) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+    for r in range(2):
+        assert not isinstance(res[r], str), res[r]
+        np.testing.assert_allclose(res[r][0], hs, rtol=1e-8)
+        assert res[r][1] == rej
+    assert np.array_equal(res[0][0], res[1][0])
+
+
 @pytest.mark.parametrize("R", [2, 3, 5])
 def test_rank_plans_sum_to_the_operator(tiny_sim, tiny_golden, R):
     """Packed per-rank plans (numpy emulation of the kernels), shared low-rank
