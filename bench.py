@@ -220,7 +220,7 @@ def accuracy_study(sim, op, nrep, precisions=("bf16",), marks=(50, 100, 200, 500
     """Relative L2 errors of slip, V, psi and theta of each precision against the FP64
     operator at equal times (dt replay of the FP64 run), after each mark; plus the FP64
     chaos floor: the same errors between two FP64 runs whose initial shear tractions
-    differ by a relative 1e-12.  The FP64 device path itself is pinned to the oracle's
+    (both components) differ by a relative 1e-12.  The FP64 device path itself is pinned to the oracle's
     simu_forward on the same operator (the cpu_baseline leg and the GPU tests)."""
     import torch
     from pyquake3d_b200.qdsim import DeviceStepper
@@ -240,7 +240,8 @@ def accuracy_study(sim, op, nrep, precisions=("bf16",), marks=(50, 100, 200, 500
     ref = DeviceStepper(sim, op, "fp64")
     others = {p: DeviceStepper(sim, op, p) for p in precisions if p in op.plans}
     pert = DeviceStepper(sim, op, "fp64")
-    pert.t["Tt1o"].mul_(1.0 + 1e-12)
+    pert.t["Tt1o"].mul_(1.0 + 1e-12)           # both shear components: a pure-dip or pure-strike
+    pert.t["Tt2o"].mul_(1.0 + 1e-12)           # fault has one of them zero
     for st in [ref, pert] + list(others.values()):
         st.ctrl[0] = sim.htry
     ref.set_history(nrep)
@@ -264,6 +265,90 @@ def accuracy_study(sim, op, nrep, precisions=("bf16",), marks=(50, 100, 200, 500
         done = mk
     out["method"] = "dt replay of the FP64 run; relative L2 over elements"
     out["sim_time_s"] = float(ref.hist.view(-1, 6)[done - 1, 2])
+    return out
+
+
+def time_stepper(stepper, k, dttry, G=100):
+    """k device-controlled steps (CUDA-graph replays of G steps when k is a multiple
+    of G): seconds by CUDA events, and the next trial size."""
+    import torch
+    g = stepper.capture(G) if k % G == 0 and k >= G else None
+    if g is None:
+        stepper.set_history(k)
+    stepper.ctrl[0] = dttry
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    if g is not None:
+        for _ in range(k // G):
+            g.replay()
+    else:
+        for i in range(k):
+            stepper.launch(i)
+    e1.record()
+    torch.cuda.synchronize()
+    c = stepper.ctrl.cpu().numpy()
+    if c[4] != 0:
+        raise RuntimeError("step failed with status %d" % int(c[4]))
+    return e0.elapsed_time(e1) / 1e3, float(c[0]), g is not None
+
+
+def config_study(case, prec, nsteps, cpu_budget, marks, extra=()):
+    """One of the smaller benchmark configurations at its full step count: steps/s of
+    `prec` and of the FP64 plain path, the H-matvec roofline, errors against the FP64
+    path (dt replay) at the marks, the FP64 path pinned to the oracle's simu_forward
+    on the same operator over the oracle's steps, and the oracle's CPU step rate."""
+    import torch
+    from pyquake3d_b200 import QDsim, meshgen, read_mshV2
+    from pyquake3d_b200.qdsim import DeviceStepper
+    import qd_oracle
+    d = os.path.join(tempfile.gettempdir(), "pq3d_bench_cfg_%s" % case)
+    msh, para = meshgen.make_case(case, d)
+    nodes, tris = read_mshV2(msh)
+    sim = QDsim(tris, nodes, para, precision=prec)
+    precs = tuple(dict.fromkeys((prec,) + tuple(extra) + ("fp64",)))
+    sim.tree_block.want = precs
+    op = sim.tree_block.op()
+    hbm, _ = peaks()
+    out = {"workload": case, "triangles": int(sim.xg.shape[0]), "precision": prec, "steps": nsteps,
+           "aca": "%s %s" % ("relative" if sim.Para0.get("ACA relative tolerance") == "True" else "absolute",
+                             sim.Para0.get("ACA tolerance")),
+           "dense_only": int(sum(1 for b in sim.tree_block.struct.blocks if b.aca)) == 0}
+    for p in precs:
+        st = DeviceStepper(sim, op, p)
+        _, dt, _ = time_stepper(st, 5, sim.htry)
+        t, _, graph = time_stepper(st, nsteps, dt)
+        x = st.x
+        for _ in range(5):
+            op.matvec(x, p, slots_only=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(50):
+            op.matvec(x, p, slots_only=True)
+        e1.record()
+        torch.cuda.synchronize()
+        tm = e0.elapsed_time(e1) / 1e3 / 50
+        ab = op.plan(p)["alg_bytes"]
+        out[p] = {"steps_per_s": nsteps / t, "ms_per_step": 1e3 * t / nsteps, "cuda_graph": graph,
+                  "hmatvec": {"ms": 1e3 * tm, "alg_bytes": int(ab), "GBs": ab / tm / 1e9, "frac": ab / tm / 1e9 / hbm},
+                  "sim_time_s": float(st.ctrl[2].item())}
+        del st
+    out["vs_fp64"] = {p: out[p]["steps_per_s"] / out["fp64"]["steps_per_s"] for p in precs}
+    low = [p for p in precs if p != "fp64"]
+    if low:
+        acc = accuracy_study(sim, op, nsteps, precisions=tuple(low), marks=marks)
+        out["err_vs_fp64"] = {p: acc[p] for p in low}
+        out["fp64_chaos_floor"] = acc["fp64_perturbed_1e-12"]
+    ho = export_host_operator(op)
+    crate, k, secs, ost, hs = cpu_reference_steps(ho, qd_oracle.sim_state(sim), sim.V0, sim.mu, sim.Cs, cpu_budget,
+                                                  max_steps=200, dttry=sim.htry, reltol=sim.RelTol, fix_tn=sim.fix_Tn)
+    out["cpu_baseline"] = {"value": crate, "unit": "steps/s", "cores": 1, "kind": "port",
+                           "sample": "%d steps (%.1f s): six block-loop MVMs + DP5(4), numpy FP64" % (k, secs)}
+    out["fp64_pinned_to_oracle"] = pin_fp64_to_oracle(sim, op, ost, hs)
+    out["vs_cpu"] = out[prec]["steps_per_s"] / crate
+    del ho, op
+    torch.cuda.empty_cache()
     return out
 
 
@@ -408,6 +493,7 @@ def ensemble_study(nsteps, nrep, faults=32):
     RMX = Ensemble(sims, precision="mixed", share=E64)
     RP = Ensemble(sims, precision="fp64", share=E64)
     RP.t["Tt1o"].mul_(1.0 + 1e-12)
+    RP.t["Tt2o"].mul_(1.0 + 1e-12)
     h = R64.run(nrep, h0)
     for R in (R32, RMX, RP):
         R.set_replay(torch.tensor(h[:, :, 0], device=R.op.dev))
@@ -584,7 +670,7 @@ def run_partition(args, rank, world, local):
     be = P.DeviceRowBackend(sim, st, int(b[rank]), int(b[rank + 1]), precision=args.precision, device=dev)
     torch.cuda.synchronize()
     t_asm = max_over_ranks(time.perf_counter() - t0 - t_host)
-    comm = P.TorchComm(use_dist=world > 1)
+    comm = P.TorchComm(use_dist=dist.is_initialized())
     ps = P.PartitionedStepper([be], comm, sim.RelTol, attempts=args.attempts)
     plan = be.op.plan(args.precision)
 
@@ -667,6 +753,7 @@ def run_partition(args, rank, world, local):
         "data": "synthetic",
         "config": {"workload": CASE + " (%d triangles), one fault" % sim.xg.shape[0],
                    "parallelism": "row partition x%d" % world, "precision": args.precision,
+                   "collectives": "NCCL" if dist.is_initialized() else "none (one rank, one process)",
                    "rows_per_rank": [int(b[r + 1] - b[r]) for r in range(world)],
                    "attempt_slots": args.attempts, "cuda_graph_steps": G if ok and args.steps % G == 0 else 0,
                    "l2": "inputs larger than L2 (operator %.2f GB per step over all ranks)" % (bytes_all / 1e9),
@@ -687,7 +774,7 @@ def run_partition(args, rank, world, local):
     }
     if rank == 0:
         print(json.dumps(line))
-    if world > 1:
+    if dist.is_initialized():
         dist.barrier()
         dist.destroy_process_group()
 
@@ -714,6 +801,9 @@ def main():
                     help="several GPUs: partition = one fault row-partitioned over the ranks (strong scaling, "
                          "the default for N > 1); replicas = one fault per rank")
     ap.add_argument("--attempts", type=int, default=3, help="attempt slots per partitioned step")
+    ap.add_argument("--no-configs", action="store_true", help="skip the plain2k and thrust20k configurations")
+    ap.add_argument("--config0-steps", type=int, default=2000, help="plain2k (dense FP64) steps")
+    ap.add_argument("--config1-steps", type=int, default=20000, help="thrust20k (FP32 low rank) steps")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     set_case(args.case)
@@ -729,7 +819,9 @@ def main():
 
     import torch
     import torch.distributed as dist
-    if world > 1:
+    if world > 1 or "TORCHELASTIC_RUN_ID" in os.environ:
+        # a process group whenever launched by torchrun (one rank included: the
+        # partitioned path then runs its collectives through NCCL)
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
@@ -743,6 +835,21 @@ def main():
     ensemble = None
     if not args.no_ensemble and world == 1:
         ensemble = ensemble_study(args.ensemble_steps, 200)
+        import gc
+        gc.collect()
+        torch.cuda.empty_cache()
+
+    # the two smaller configurations at their full step counts: plain2k (dense FP64
+    # operator, 2,000 steps) and thrust20k (FP32 low rank, 20,000 steps; mixed beside it)
+    configs = None
+    if not args.no_configs and world == 1:
+        configs = {}
+        for name, prec, k, marks, extra in (("plain2k", "fp64", args.config0_steps, (500, 2000), ()),
+                                            ("thrust20k", "fp32", args.config1_steps, (500, 2000, 20000), ("mixed",))):
+            try:
+                configs[name] = config_study(name, prec, k, 10.0, marks, extra=extra)
+            except RuntimeError as e:       # recorded in the line; the headline still runs
+                configs[name] = {"error": str(e)}
         import gc
         gc.collect()
         torch.cuda.empty_cache()
@@ -976,6 +1083,7 @@ def main():
         "vmode": vmode,
         "vmode_curved120k": vmode120,
         "ensemble": ensemble,
+        "configs": configs,
         "gf_assembly": gf,
         "sim": {"time_s": float(hist[-1, 2]), "last_dt": float(hist[-1, 0]), "rejects": int(hist[:, 5].sum())},
         "e2e": e2e,
@@ -986,7 +1094,7 @@ def main():
     }
     if rank == 0:
         print(json.dumps(line))
-    if world > 1:
+    if dist.is_initialized():
         dist.barrier()
         dist.destroy_process_group()
 

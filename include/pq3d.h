@@ -206,7 +206,7 @@ int pq3d_rk_rows_accept(const void *args, int grid, int r0, int r1, double h, do
  * block pc (16 doubles: [0] h of the next attempt, [1] dtnext, [2] time, [3]
  * rejects this step, [4] status, [5] accepted, [6] max|V1|, [7] max|V2|, [8]
  * steps, [9] total rejects, [10] halt, [11] first attempt pending, [12] attempts
- * this step) and receives the same maxima reduced over ranks, so all ranks decide
+ * this step, [13] accepted h of the last step) and receives the same maxima reduced over ranks, so all ranks decide
  * alike without the host.  A step is the fixed sequence attempt_dev -> reduce ->
  * control (max_attempts times), accept_dev -> reduce -> finish; kernels skip
  * their work once the step is accepted or halted.  control halts with status 0

@@ -9,8 +9,8 @@ and times each candidate with CUDA events on the launching stream:
 Coordinate descent from the current shapes, two sweeps over the three knobs;
 a candidate is kept only when it beats the best time by more than the noise
 margin.  The winners are written per GPU model and storage into the plan cache
-(pyquake3d_b200/plan_cache.json), which DeviceHMatrix reads when it builds a
-plan.
+(pyquake3d_b200/plan_cache.json), one entry per workload size; DeviceHMatrix
+reads the entry tuned on the size closest to its own when it builds a plan.
 
     python -m pyquake3d_b200.autotune --case curved60k --precisions fp32,mixed,fp64 \
         [--out plan_cache.json]
@@ -115,9 +115,13 @@ def main():
         default = [r for r in trials if (r["dense_chunk"], r["v_chunk"], r["u_rows"]) ==
                    (op.DENSE_CHUNK_GROUPS[{"fp64": 0, "fp32": 1, "bf16": 2, "mixed": 3}[p]],
                     op.V_CHUNK_GROUPS[{"fp64": 0, "fp32": 1, "bf16": 2, "mixed": 3}[p]], op.U_ROWS)]
-        ent[p] = dict(shapes, us=round(1e6 * t, 1), workload="%s (%d triangles)" % (args.case, op.n),
-                      default_us=round(1e3 * default[0]["ms"], 1) if default else None, trials=len(trials))
-        print(json.dumps({p: ent[p]}))
+        new = dict(shapes, us=round(1e6 * t, 1), workload="%s (%d triangles)" % (args.case, op.n), n=int(op.n),
+                   default_us=round(1e3 * default[0]["ms"], 1) if default else None, trials=len(trials))
+        # one entry per workload size: replace this workload's, keep the others'
+        old = ent.get(p)
+        olds = [] if old is None else ([old] if isinstance(old, dict) else list(old))
+        ent[p] = [e for e in olds if e.get("workload") != new["workload"]] + [new]
+        print(json.dumps({p: new}))
     with open(out, "w") as f:
         json.dump(cache, f, indent=1, sort_keys=True)
     print("plan cache:", out)

@@ -327,7 +327,8 @@ enum {
     PC_STEPS = 8, PC_REJ = 9,
     PC_HALT = 10,    // no further work until the host resumes
     PC_FIRST = 11,   // the next attempt is the step's first (sums the matvec slots)
-    PC_ATT = 12      // attempts in this step
+    PC_ATT = 12,     // attempts in this step
+    PC_LASTH = 13    // accepted h of the last step
 };
 
 __global__ void __launch_bounds__(RK_THREADS) k_rk_rows_attempt_dev(RkArgs A, int r0, int r1, const double *pc,
@@ -403,6 +404,7 @@ __global__ void k_rk_rows_finish(double *pc, const double *V8)
     pc[PC_REJ] += pc[PC_NRJCT];
     pc[PC_V1] = V8[0];
     pc[PC_V2] = V8[1];
+    pc[PC_LASTH] = pc[PC_H];
     pc[PC_H] = pc[PC_DTNEXT];
     pc[PC_NRJCT] = 0.0;
     pc[PC_ACC] = 0.0;

@@ -573,9 +573,19 @@ PLAN_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "plan_cach
 _plan_cache = None
 
 
-def plan_cache_entry(gpu_name, dtype):
+def _entry_n(e):
+    """Element count of the workload a cache entry was tuned on."""
+    if "n" in e:
+        return int(e["n"])
+    import re
+    m = re.search(r"\((\d+) triangles\)", e.get("workload", ""))
+    return int(m.group(1)) if m else None
+
+
+def plan_cache_entry(gpu_name, dtype, n=None):
     """Work-item shapes measured by pyquake3d_b200.autotune for this GPU model and
-    storage, or None."""
+    storage, or None.  The cache may hold entries tuned on workloads of several
+    sizes (a list); the one tuned on the size closest to n (log scale) is used."""
     global _plan_cache
     if _plan_cache is None:
         _plan_cache = {}
@@ -583,7 +593,13 @@ def plan_cache_entry(gpu_name, dtype):
             import json
             with open(PLAN_CACHE) as f:
                 _plan_cache = json.load(f)
-    return _plan_cache.get(gpu_name, {}).get(dtype)
+    ent = _plan_cache.get(gpu_name, {}).get(dtype)
+    if ent is None or isinstance(ent, dict):
+        return ent
+    sized = [e for e in ent if _entry_n(e)]
+    if n is None or not sized:
+        return ent[0] if ent else None
+    return min(sized, key=lambda e: abs(np.log(_entry_n(e) / float(n))))
 
 
 # ----------------------------------------------------------------------------- device operator
@@ -836,7 +852,7 @@ class DeviceHMatrix:
         if ov is not None:
             return ov
         if self.use_plan_cache:
-            ent = plan_cache_entry(self.torch.cuda.get_device_name(self.dev), dtype)
+            ent = plan_cache_entry(self.torch.cuda.get_device_name(self.dev), dtype, self.n)
             if ent is not None:
                 return int(ent["dense_chunk"]), int(ent["v_chunk"]), int(ent["u_rows"])
         return self.DENSE_CHUNK_GROUPS[code], self.V_CHUNK_GROUPS[code], self.U_ROWS

@@ -233,10 +233,19 @@ class TorchComm:
             self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return t
 
+    def max_inplace(self, parts):
+        """max, reduced into the one local part itself when there is one (no copy);
+        the caller reads it before that buffer is written again."""
+        if len(parts) != 1:
+            return self.max(parts)
+        if self.use_dist:
+            self.dist.all_reduce(parts[0], op=self.dist.ReduceOp.MAX)
+        return parts[0]
+
 
 # control block of the device-controlled step (pq3d_rk_rows_control, include/pq3d.h)
 PC_H, PC_DTNEXT, PC_TIME, PC_NRJCT, PC_STATUS, PC_ACC, PC_V1, PC_V2, PC_STEPS, PC_REJ, PC_HALT, PC_FIRST, PC_ATT = range(13)
-PC_LASTH = 13          # kept on the host side of the record: the last accepted h (written by pc_resume / finish)
+PC_LASTH = 13          # accepted h of the last step (pq3d_rk_rows_finish, or the host after a halted step)
 
 
 def _nan_encode(v):
@@ -330,10 +339,10 @@ class PartitionedStepper:
         for b in self.backends:
             b.matvec_gathered(xt)
         for _ in range(self.attempts):
-            E = self.comm.max([b.attempt_dev() for b in self.backends])
+            E = self.comm.max_inplace([b.attempt_dev() for b in self.backends])
             for b in self.backends:
                 b.control(E, self.reltol, self.attempts)
-        V = self.comm.max([b.accept_dev() for b in self.backends])
+        V = self.comm.max_inplace([b.accept_dev() for b in self.backends])
         for b in self.backends:
             b.finish(V)
 
@@ -536,19 +545,24 @@ class DeviceRowBackend:
                                               ptr(self.out), _lib.stream_ptr()), "pq3d_rk_rows_attempt_dev")
         return self.out
 
-    def control(self, E, reltol, attempts):
-        # the reduced maxima may live in a buffer the next reduction reuses: keep a copy
+    def _reduced(self, E):
+        """The reduced maxima where the control kernels read them: this rank's own
+        output buffer when the reduction ran in place, else a copy (a buffer of the
+        communicator's may be reused by the next reduction)."""
+        if E.data_ptr() == self.out.data_ptr():
+            return self.out
         self.E8.copy_(E)
-        check(self.L.pq3d_rk_rows_control(ptr(self.pc), ptr(self.E8), float(reltol), int(attempts),
+        return self.E8
+
+    def control(self, E, reltol, attempts):
+        check(self.L.pq3d_rk_rows_control(ptr(self.pc), ptr(self._reduced(E)), float(reltol), int(attempts),
                                           _lib.stream_ptr()), "pq3d_rk_rows_control")
 
     def accept_dev(self):
-        # the accepted h, for the host record, before finish replaces pc[PC_H] by dtnext
-        self.pc[PC_LASTH:PC_LASTH + 1].copy_(self.pc[PC_H:PC_H + 1])
         check(self.L.pq3d_rk_rows_accept_dev(self.args.ctypes.data, self.grid, self.r0, self.r1, ptr(self.pc),
                                              ptr(self.out), _lib.stream_ptr()), "pq3d_rk_rows_accept_dev")
         return self.out
 
     def finish(self, V):
-        self.E8.copy_(V)
-        check(self.L.pq3d_rk_rows_finish(ptr(self.pc), ptr(self.E8), _lib.stream_ptr()), "pq3d_rk_rows_finish")
+        check(self.L.pq3d_rk_rows_finish(ptr(self.pc), ptr(self._reduced(V)), _lib.stream_ptr()),
+              "pq3d_rk_rows_finish")

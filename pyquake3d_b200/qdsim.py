@@ -25,6 +25,8 @@ behaviour by default):
 import ctypes
 import math
 import os
+import queue
+import threading
 import weakref
 
 import numpy as np
@@ -498,6 +500,89 @@ class HostEvent:
         return rc == 1
 
 
+class _CopyJob:
+    """The host copies of one step's prefetched vectors, filled by _PrefetchCopier."""
+
+    def __init__(self, names):
+        self.names = names
+        self.out = {}
+        self.ready = {nm: threading.Event() for nm in names}
+        self.taken = set()
+        self.error = None
+
+    def has(self, name):
+        return name in self.ready and name not in self.taken
+
+    def get(self, name):
+        self.taken.add(name)
+        self.ready[name].wait()
+        if self.error is not None:
+            raise self.error
+        return self.out.pop(name)
+
+    def wait_all(self):
+        for ev in self.ready.values():
+            ev.wait()
+
+
+class _PrefetchCopier:
+    """A host thread that turns each step's prefetched state vectors (pinned host
+    memory, written by the copy engine after the step) into the fresh arrays the
+    reference main loop reads and keeps (np.max(np.abs(sim0.slipv1)),
+    SLIPV.append(sim0.slipv), src/main.py:168-184).  It waits for the copy to land,
+    then copies each vector into an array whose pages it touched beforehand, while
+    the device already runs the next step's H-matvec: first touches of fresh memory
+    (the loop keeps every array, so none is reused) cost the caller's thread more
+    than the copy.  A read then waits only for its own vector."""
+
+    def __init__(self, n, device_index, spare=8):
+        self.n = n
+        self.q = queue.Queue()
+        self.spare = []
+        self.keep = spare
+        self.thread = threading.Thread(target=self._run, args=(device_index,), daemon=True)
+        self.thread.start()
+
+    def submit(self, done, views, names):
+        job = _CopyJob(names)
+        self.q.put((job, done, views))
+        return job
+
+    def stop(self):
+        self.q.put(None)
+
+    def _fresh(self):
+        if self.spare:
+            return self.spare.pop()
+        a = np.empty(self.n)
+        ctypes.memset(a.ctypes.data, 0, a.nbytes)        # first touch, without the GIL
+        return a
+
+    def _run(self, device_index):
+        import torch
+        torch.cuda.set_device(device_index)
+        while True:
+            item = self.q.get()
+            if item is None:
+                return
+            job, done, views = item
+            try:
+                done.synchronize()
+                for nm in job.names:
+                    a = self._fresh()
+                    np.copyto(a, views[nm])
+                    job.out[nm] = a
+                    job.ready[nm].set()
+            except Exception as e:          # handed to the reader
+                job.error = e
+            for ev in job.ready.values():
+                ev.set()
+            while len(self.spare) < self.keep and self.q.empty():
+                a = np.empty(self.n)
+                ctypes.memset(a.ctypes.data, 0, a.nbytes)
+                self.spare.append(a)
+
+
 class _StepGraph:
     """CUDA graph of consecutive steps.  A replay rewrites the operator's slots
     and advances the state, so it invalidates pre-launched products and the
@@ -557,7 +642,8 @@ class DeviceStepper:
         self._io = None                 # mapped control block and step event (step())
         self._state_event = False       # step_done marks the current state (no launch since)
         self._snaps = {}                # snapshot buffers per tuple of names
-        self._prefetched = None         # (done event, views) of the last step's prefetch
+        self._prefetched = None         # _CopyJob of the last step's prefetch
+        self._copier = None             # _PrefetchCopier, started by the first prefetch
         self.x = op.new_x(precision)
         from .hmatrix import pack_x
         x0 = pack_x((sim.slipv1 - sim.slipvC * np.cos(sim.rake0))[self.perm],
@@ -658,7 +744,12 @@ class DeviceStepper:
         if pre is not None:
             # only the next step kernel (which writes the state) waits for the gather
             check(L.pq3d_stream_wait_event(stream, pre[2]), "pq3d_stream_wait_event")
-            self._prefetched = (pre[0], pre[1])
+            if self._copier is None:
+                self._copier = _PrefetchCopier(self.n, self.op.dev.index or 0)
+                weakref.finalize(self, self._copier.stop)
+            self._prefetched = self._copier.submit(pre[0], pre[1], prefetch)
+            S = self._snaps[tuple(prefetch)]
+            S["jobs"][S["k"] ^ 1] = self._prefetched      # reads that buffer until done
         check(L.pq3d_event_sync(io["step_done"]), "pq3d_event_sync")
         c = io["ctrl"]
         if c[15] != self.steps + 1:
@@ -759,11 +850,15 @@ class DeviceStepper:
                  "fields": np.array([self.t[nm].data_ptr() for nm in names], dtype=np.uint64),
                  "stage": [torch.empty(nf * n, dtype=torch.float64, device=self.op.dev) for _ in range(2)],
                  "host": hosts, "views": views, "gathered": events[0::2],
-                 "done": [HostEvent(L, e) for e in events[1::2]]}
+                 "done": [HostEvent(L, e) for e in events[1::2]], "jobs": [None, None]}
             S["release"] = weakref.finalize(self, _release_host_io, L, hosts, events)
             self._snaps[names] = S
         b = S["k"]
         S["k"] ^= 1
+        job = S["jobs"][b]
+        if job is not None:
+            job.wait_all()                  # the host copier still reads this buffer
+            S["jobs"][b] = None
         compute = _lib.stream_ptr()
         io = self._io if self._io is not None else self._host_io()
         if not self._state_event:
@@ -788,9 +883,8 @@ class DeviceStepper:
         from that step's prefetch when it holds the vector and nothing was launched
         since, else by a snapshot of its own."""
         pf = self._prefetched
-        if pf is not None and name in pf[1]:
-            pf[0].synchronize()
-            return np.array(pf[1][name])
+        if pf is not None and pf.has(name):
+            return pf.get(name)
         return self.fetch((name,))[name]
 
     def get(self, name):

@@ -120,7 +120,6 @@ class NumpyRowBackend:
     def accept_dev(self):
         from pyquake3d_b200 import partition as P
         pc = self.pc
-        pc[P.PC_LASTH] = pc[P.PC_H]
         if pc[P.PC_HALT] == 0 and pc[P.PC_ACC] != 0:
             self.out = self.accept(float(pc[P.PC_H]))
         return self.out
@@ -134,6 +133,7 @@ class NumpyRowBackend:
         pc[P.PC_STEPS] += 1
         pc[P.PC_REJ] += pc[P.PC_NRJCT]
         pc[P.PC_V1], pc[P.PC_V2] = V8[0], V8[1]
+        pc[P.PC_LASTH] = pc[P.PC_H]
         pc[P.PC_H] = pc[P.PC_DTNEXT]
         pc[P.PC_NRJCT] = pc[P.PC_ACC] = pc[P.PC_ATT] = 0
         pc[P.PC_FIRST] = 1

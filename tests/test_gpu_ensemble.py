@@ -108,8 +108,9 @@ def test_full_32_fault_deck_fp32_and_mixed_within_target_or_chaos_floor(tmp_path
     runs = {}
     for name, prec in (("fp32", "fp32"), ("mixed", "mixed"), ("floor", "fp64")):
         R = Ensemble(sims, precision=prec, share=E64)
-        if name == "floor":
+        if name == "floor":                    # both shear components (a pure-dip fault has Tt1o = 0)
             R.t["Tt1o"].mul_(1.0 + 1e-12)
+            R.t["Tt2o"].mul_(1.0 + 1e-12)
         R.set_replay(torch.tensor(h[:, :, 0], device=R.op.dev))
         R.run(nrep, h0)
         runs[name] = R

@@ -132,7 +132,7 @@ def test_reference_loop_reads_current_state(lib, tiny_files):
     sim = QDsim(tris, nodes, tiny_files[1])
     v0 = sim.slipv.copy()
     dttry = sim.htry
-    slipv_hist = []
+    slipv_hist, copies = [], []
     for i in range(6):
         dttry, dtnext = sim.simu_forward(dttry)
         st = sim._dev
@@ -143,7 +143,11 @@ def test_reference_loop_reads_current_state(lib, tiny_files):
         for name, dev in (("slipv", "slipv"), ("Tt", "Tt"), ("state", "psi"), ("slip", "slip")):
             assert np.array_equal(getattr(sim, name), st.get(dev)), (i, name)
         slipv_hist.append(sim.slipv)
+        copies.append(st.get("slipv"))
         dttry = dtnext
+    # the kept arrays are the host copier's fresh arrays: later steps leave them alone
+    for i, (a, b) in enumerate(zip(slipv_hist, copies)):
+        assert np.array_equal(a, b), i
     assert not np.array_equal(slipv_hist[0], v0)
     assert not np.array_equal(slipv_hist[0], slipv_hist[-1])
     assert len({id(a) for a in slipv_hist}) == len(slipv_hist)

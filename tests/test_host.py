@@ -60,3 +60,23 @@ def test_seeded_aca_starts_match_reference_draws(tiny_sim, tiny_golden):
         m, n = len(b.row.indices), len(b.col.indices)
         assert s == (np.random.randint(m) - 3, np.random.randint(n) - 3)
         assert d == (np.random.randint(m) - 3, np.random.randint(n) - 3)
+
+
+def test_plan_cache_picks_entry_of_nearest_size(tmp_path, monkeypatch):
+    """Work-item shapes: the autotuner's entry tuned on the workload size closest to
+    the operator's (log scale); a single-entry cache (older form) still reads."""
+    import json
+    from pyquake3d_b200 import hmatrix
+    cache = {"GPU X": {"fp32": [dict(dense_chunk=4, v_chunk=8, u_rows=256, workload="plain2k (1936 triangles)"),
+                                dict(dense_chunk=16, v_chunk=64, u_rows=512, n=59696)],
+                       "mixed": dict(dense_chunk=16, v_chunk=64, u_rows=512, workload="curved60k (59696 triangles)")}}
+    p = tmp_path / "plan_cache.json"
+    p.write_text(json.dumps(cache))
+    monkeypatch.setattr(hmatrix, "PLAN_CACHE", str(p))
+    monkeypatch.setattr(hmatrix, "_plan_cache", None)
+    assert hmatrix.plan_cache_entry("GPU X", "fp32", 2000)["dense_chunk"] == 4
+    assert hmatrix.plan_cache_entry("GPU X", "fp32", 20480)["dense_chunk"] == 16
+    assert hmatrix.plan_cache_entry("GPU X", "fp32", 120000)["dense_chunk"] == 16
+    assert hmatrix.plan_cache_entry("GPU X", "mixed", 2000)["v_chunk"] == 64
+    assert hmatrix.plan_cache_entry("GPU X", "bf16", 2000) is None
+    assert hmatrix.plan_cache_entry("GPU Y", "fp32", 2000) is None
