@@ -25,6 +25,7 @@
 //   k_u         (FP64) the U tasks as a plain launch after k_dense_v.
 //   k_rowsum    y[i] = sum of row i's slots (FP64), plus optional loading terms
 //               (skipped when the step kernel sums the slots itself)
+#include <algorithm>
 #include "pq3d_common.cuh"
 #include "hm_layout.cuh"
 #include <cuda_bf16.h>
@@ -498,20 +499,41 @@ __device__ __forceinline__ void u_task_mixed(const UTaskM &T, const float *__res
     }
 }
 
-// V items of all three classes, one warp each (the class picks the element type).
+// V items of all three classes (the class picks the element type).  Persistent: the
+// grid is the resident CTAs, and every warp works through items w, w + W, w + 2W, ...
+// (W warps in the grid) on its own, with no barrier, so a CTA never holds its slot
+// for its slowest warp.  The host sorts the items by size, largest first, so the
+// strides leave every warp about the same work.  The mixed storage has many small V
+// items (a block's terms split three ways), which one-item-per-warp CTAs left
+// uneven: at 20k the SMs were busy 64% of the kernel's time.
 __global__ void __launch_bounds__(256, PQ3D_VMIX_MINB)
 k_v_mixed(const VItem *__restrict__ vitems, int64_t n_vitems, const float *__restrict__ V32,
           const __half *__restrict__ V16, const uint8_t *__restrict__ V8, const float *__restrict__ x, int xstride,
           float *__restrict__ tpart)
 {
     asm volatile("griddepcontrol.launch_dependents;");
-    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (w >= n_vitems) return;
-    const VItem it = vitems[w];
-    const int cls = it.s >> 8, slip = it.s & 255;
-    if (cls == 0) v_item<float, float>(it, slip, V32, x, xstride, tpart);
-    else if (cls == 1) v_item<__half, float>(it, slip, V16, x, xstride, tpart);
-    else v_item<uint8_t, float>(it, slip, V8, x, xstride, tpart);
+    const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < n_vitems; w += nw) {
+        const VItem it = vitems[w];
+        const int cls = it.s >> 8, slip = it.s & 255;
+        if (cls == 0) v_item<float, float>(it, slip, V32, x, xstride, tpart);
+        else if (cls == 1) v_item<__half, float>(it, slip, V16, x, xstride, tpart);
+        else v_item<uint8_t, float>(it, slip, V8, x, xstride, tpart);
+    }
+}
+
+// Resident CTAs of k_v_mixed on the current device (its persistent grid), per device.
+static int vmix_ctas()
+{
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (dev >= 0 && dev < 64 && cached[dev] > 0) return cached[dev];
+    int sms = 0, per = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_v_mixed, 256, 0) != cudaSuccess || per <= 0) return 0;
+    if (dev >= 0 && dev < 64) cached[dev] = sms * per;
+    return sms * per;
 }
 
 // Dense items, then the mixed U tasks (programmatic dependent launch after k_v_mixed,
@@ -1135,7 +1157,9 @@ static int run_matvec_mixed(const HmPlan &P, const float *x, float *slots, float
                             const double *add1, const double *add2, double *y, cudaStream_t st)
 {
     if (P.n_vitems > 0) {
-        const int64_t blocks = (P.n_vitems * 32 + 255) / 256;
+        const int resident = vmix_ctas();
+        if (resident <= 0) return PQ3D_ERR_CUDA;
+        const int64_t blocks = std::min<int64_t>((P.n_vitems * 32 + 255) / 256, resident);
         k_v_mixed<<<(unsigned)blocks, 256, 0, st>>>((const VItem *)P.vitems, P.n_vitems, (const float *)P.V,
                                                     (const __half *)P.V16, (const uint8_t *)P.V8, x, x_stride(P.n),
                                                     tpart);

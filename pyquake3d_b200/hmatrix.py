@@ -440,6 +440,9 @@ def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chu
     A = _leaf_lists(struct, slot_rows)
     dense_entries = int(np.sum(dense_recs["m"].astype(np.int64) * dense_recs["n"])) if len(dense_recs) else 0
     n = struct.n
+    if not stream:
+        # k_v_mixed's warps stride through the items: largest first evens out their work
+        vitems.sort(key=lambda v: -v[3] * (v[5] - v[4]))
     A.update(ditems=_rec(ditems, _lib.DENSE_ITEM), vitems=_rec(vitems, _lib.V_ITEM),
              utasks=_rec(utasks, _lib.U_TASK_M), n_ditems=len(ditems), n_vitems=len(vitems), n_utasks=len(utasks),
              n_slots=slot, n_tpart=tp, n_scales=sb, kmax=kmax, u_sizes=u_off, v_sizes=v_off, pack=pack, stream=stream,
