@@ -101,6 +101,18 @@ def gf_roofline(op, struct):
     del out32, out64
     out = {"kernel": "k_dense_assemble (full space)", "pairs": pairs, "ms": 1e3 * t,
            "pair_evals_per_s": 2 * pairs / t}
+    # ACA (k_aca): every iteration of a slip pass evaluates one residual row (n
+    # sources) and one column (m receivers) of the block's Green's function, so a pass
+    # of rank k costs at least k (m + n) single-slip pair evaluations (reference-set
+    # resets add more): a lower bound on its rate, against the dense assembly's
+    kS, kD = op.ranks()
+    mn = np.array([len(b.row.indices) + len(b.col.indices) for b in struct.blocks if b.aca], dtype=np.float64)
+    aca_pairs = float(np.sum((kS + kD) * mn))
+    aca_s = op.timings.get("aca_s")
+    if aca_s:
+        out["aca"] = {"pair_evals_min": aca_pairs, "s": aca_s, "pair_evals_per_s_min": aca_pairs / aca_s,
+                      "vs_dense_rate_min": aca_pairs / aca_s / (2 * pairs / t),
+                      "note": "lower bound: k (m + n) single-slip evaluations per pass of rank k"}
     fp = os.path.join(REPO, "profiles", "gf_flops.json")
     if os.path.exists(fp):
         f = json.load(open(fp))

@@ -154,7 +154,9 @@ int pq3d_aca_pack_mixed(const void *d_tasks, int64_t n_tasks, const double *d_ws
 /* ---------------------------------------------------------------- H-matvec */
 
 /* Sizes of the work-item records: kind 0 DenseItem, 1 VItem, 2 UTask,
- * 4 DenseBlock, 5 the plan struct, 6 the mixed-storage U task. */
+ * 4 DenseBlock, 5 the plan struct, 6 the mixed-storage U task, 7 and 8 the
+ * streamed kernels' task and t-gather records, 9 the mixed-storage V item (rows
+ * of the blocks that share a column cluster), 10 its row record. */
 size_t pq3d_item_bytes(int kind);
 
 /* y (n x 3, FP64) = [A1s A1d; A2s A2d; Bs Bd] x (+ add0/add1/add2 per component).
@@ -172,6 +174,9 @@ int pq3d_hmatvec(const void *plan_host, const void *d_x, void *d_slots, void *d_
 /* Resident CTAs of the bulk-copy (streamed) mixed-storage kernel on the current
  * device: the persistent grid its task lists are balanced for. */
 int pq3d_stream_ctas(void);
+/* Resident CTAs of the mixed storage's V kernel on the current device: a plan's
+ * per-warp V item lists are made for 8 warps per resident CTA. */
+int pq3d_vmix_ctas(void);
 
 /* ---------------------------------------------------------------- stepper */
 

@@ -20,6 +20,10 @@ i32 = ctypes.c_int
 DENSE_BLOCK = np.dtype([("off64", "i8"), ("off32", "i8"), ("m", "i4"), ("n", "i4"), ("r0", "i4"), ("c0", "i4")], align=True)
 DENSE_ITEM = np.dtype([("off", "i8"), ("m", "i4"), ("r", "i4"), ("g0", "i4"), ("g1", "i4"), ("c0", "i4"), ("slot", "i4")], align=True)
 V_ITEM = np.dtype([("off", "i8"), ("Q", "i4"), ("q", "i4"), ("nr", "i4"), ("g0", "i4"), ("g1", "i4"), ("c0", "i4"), ("s", "i4"), ("tp", "i4")], align=True)
+# mixed storage, plain kernels: merged V items over the rows of blocks sharing a column cluster
+V_ITEM_M = np.dtype([("rows", "i8"), ("nr", "i4"), ("g0", "i4"), ("g1", "i4"), ("c0", "i4"), ("s", "i4"), ("pad", "i4")],
+                    align=True)
+V_ROW = np.dtype([("base", "i8"), ("stride", "i4"), ("out", "i4")], align=True)
 U_TASK = np.dtype([("off", "i8"), ("m", "i4"), ("r0", "i4"), ("r1", "i4"), ("K", "i4"), ("kS", "i4"), ("kD", "i4"), ("Q", "i4"), ("tp", "i4"), ("nch", "i4"), ("slot", "i4")], align=True)
 ACA_TASK = np.dtype([("rows_off", "i8"), ("cols_off", "i8"), ("ws_off", "i8"), ("m", "i4"), ("n", "i4"), ("kmax", "i4"), ("pass_", "i4"), ("iref0", "i4"), ("jref0", "i4")], align=True)
 PACK_TASK = np.dtype([("ws_off", "i8"), ("u_off", "i8"), ("v_off", "i8"), ("rows_off", "i8"), ("cols_off", "i8"),
@@ -32,7 +36,8 @@ HM_PLAN = np.dtype([("n", "i4"), ("dtype", "i4")] + [(p, "u8") for p in _PLAN_PT
                    [(p, "u8") for p in ("U16", "V16", "U8", "V8", "scales", "status")] +
                    [("stream", "i4"), ("pad2", "i4")] +
                    [(p, "u8") for p in ("tasks_a", "tasks_b", "cta_a", "cta_b", "gather", "tfull")] +
-                   [("n_gather", "i8"), ("ncta_a", "i4"), ("ncta_b", "i4")], align=True)
+                   [("n_gather", "i8"), ("ncta_a", "i4"), ("ncta_b", "i4"), ("vrows", "u8"), ("vwarp", "u8"),
+                    ("n_vwarp", "i4"), ("pad3", "i4")], align=True)
 # streamed mixed kernels (k_stream in hmatvec.cu): stage bytes, shared x/t buffer (floats),
 # the row limits of dense and U tasks
 STREAM_STAGE_BYTES, STREAM_BUF, STREAM_DENSE_ROWS, STREAM_ROWS = 12288, 3072, 128, 256
@@ -118,6 +123,7 @@ def load():
     L.pq3d_hmatvec.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.pq3d_pack_mixed_task_bytes.restype = ctypes.c_size_t
     L.pq3d_stream_ctas.restype = ctypes.c_int
+    L.pq3d_vmix_ctas.restype = ctypes.c_int
     L.pq3d_nearfield_rowabs.argtypes = [vp, vp, i64, i32, vp, vp]
     L.pq3d_aca_term_weights.argtypes = [vp, i64, vp, vp, vp, vp, vp, vp]
     L.pq3d_aca_pack_mixed.argtypes = [vp, i64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
@@ -153,6 +159,7 @@ def load():
              "UTask": (L.pq3d_item_bytes(2), U_TASK.itemsize), "UTaskM": (L.pq3d_item_bytes(6), U_TASK_M.itemsize),
              "PackTaskM": (L.pq3d_pack_mixed_task_bytes(), PACK_TASK_M.itemsize),
              "StreamTask": (L.pq3d_item_bytes(7), STREAM_TASK.itemsize), "TGather": (L.pq3d_item_bytes(8), T_GATHER.itemsize),
+             "VItemM": (L.pq3d_item_bytes(9), V_ITEM_M.itemsize), "VRowRec": (L.pq3d_item_bytes(10), V_ROW.itemsize),
              "DenseBlock": (L.pq3d_item_bytes(4), DENSE_BLOCK.itemsize), "HmPlan": (L.pq3d_item_bytes(5), HM_PLAN.itemsize),
              "AcaTask": (L.pq3d_aca_task_bytes(), ACA_TASK.itemsize), "PackTask": (L.pq3d_pack_task_bytes(), PACK_TASK.itemsize),
              "RkArgs": (L.pq3d_rk_args_bytes(), RK_ARGS.itemsize),

@@ -67,6 +67,15 @@ struct VItem {              // V rows [q, q+nr) (nr <= 32, one slip) of a block,
     int64_t off;            // block offset in the V array
     int32_t Q, q, nr, g0, g1, c0, s, tp;  // s: slip of these rows; tp: this chunk's partial t (Q values)
 };
+struct VItemM {             // mixed storage: rows [rows, rows + nr) (nr <= 32) of the VRowRec list,
+    int64_t rows;           // one class and one slip, from the low-rank blocks that share one
+    int32_t nr, g0, g1, c0, s, pad;  // column cluster; column groups [g0, g1); s: slip | class << 8
+};
+struct VRowRec {            // one V row of a VItemM
+    int64_t base;           // element offset of (column group 0, this row) in its class array
+    int32_t stride;         // elements per column group of its block (Q * CW)
+    int32_t out;            // index of this row's chunk partial in t
+};
 struct UTask {              // one CTA: rows [r0, r1) of a low-rank block
     int64_t off;            // block offset in the U array
     int32_t m, r0, r1, K, kS, kD, Q, tp, nch, slot;  // tp/nch: the block's chunk partials of t (stride Q)

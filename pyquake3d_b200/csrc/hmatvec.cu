@@ -499,26 +499,93 @@ __device__ __forceinline__ void u_task_mixed(const UTaskM &T, const float *__res
     }
 }
 
+// A merged V item of the mixed storage: up to 32 rows (one class, one slip) taken from
+// the low-rank blocks that share one column cluster, so their x slice is loaded once
+// for all of them.  Lanes and summation order are those of v_item (8 rows x 4 column
+// groups per warp load, up to 4 rows per lane, groups jg, jg + 4, ... per lane, then a
+// 2-step shuffle reduction), so each row's sum is the one v_item forms for it.
+template <typename TL>
+__device__ __forceinline__ void v_item_m(const VItemM &it, int slip, const TL *__restrict__ Vd,
+                                         const VRowRec *__restrict__ recs, const float *__restrict__ x, int xstride,
+                                         float *__restrict__ tpart)
+{
+    constexpr int CWV = 16 / sizeof(TL);
+    const int lane = threadIdx.x & 31;
+    const int rr = lane & 7, jg = lane >> 3;
+    const int nu = rr < it.nr ? (it.nr - rr + 7) >> 3 : 0;    // rows of this lane (0..4)
+    // element offsets in the class array (the host keeps every class array below 2^32
+    // elements), one register per row instead of a pointer's two
+    uint32_t off[4];
+    int32_t st4[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        off[u] = 0;
+        st4[u] = 0;
+        if (u < nu) {
+            const VRowRec R = recs[it.rows + rr + 8 * u];
+            off[u] = (uint32_t)(R.base + (int64_t)(it.g0 + jg) * R.stride);
+            st4[u] = 4 * R.stride;
+        }
+    }
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    if (nu > 0) {
+        const float *xp = x + (int64_t)(2 + slip) * xstride + it.c0 + (int64_t)(it.g0 + jg) * CWV;  // CWV-aligned
+#pragma unroll 2
+        for (int g = it.g0 + jg; g < it.g1; g += 4) {
+            float xs[CWV];
+            ld_vec<float, CWV>(xp, xs);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (u < nu) {
+                    Vec16<TL> d = ld_stream(Vd + off[u]);
+                    if constexpr (std::is_same<TL, uint8_t>::value) {
+#pragma unroll
+                        for (int t = 0; t < 4; ++t) {
+                            acc[u] += i8_at<0>(d.w[t]) * xs[4 * t];
+                            acc[u] += i8_at<1>(d.w[t]) * xs[4 * t + 1];
+                            acc[u] += i8_at<2>(d.w[t]) * xs[4 * t + 2];
+                            acc[u] += i8_at<3>(d.w[t]) * xs[4 * t + 3];
+                        }
+                    } else {
+#pragma unroll
+                        for (int t = 0; t < CWV; ++t) acc[u] += widen<float>(d.v[t]) * xs[t];
+                    }
+                    off[u] += st4[u];
+                }
+            }
+            xp += 4 * CWV;
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], 8);
+        acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], 16);
+        if (jg == 0 && u < nu) tpart[recs[it.rows + rr + 8 * u].out] = acc[u];
+    }
+}
+
 // V items of all three classes (the class picks the element type).  Persistent: the
-// grid is the resident CTAs, and every warp works through items w, w + W, w + 2W, ...
-// (W warps in the grid) on its own, with no barrier, so a CTA never holds its slot
-// for its slowest warp.  The host sorts the items by size, largest first, so the
-// strides leave every warp about the same work.  The mixed storage has many small V
-// items (a block's terms split three ways), which one-item-per-warp CTAs left
-// uneven: at 20k the SMs were busy 64% of the kernel's time.
+// grid is the resident CTAs, and warp w works through its own list of items
+// [vwarp[w], vwarp[w + 1]) with no barrier, so a CTA never holds its slot for its
+// slowest warp.  The host fills the lists largest item first, each into the least
+// loaded warp, so the warps end together.  (One item per warp, as CTAs of 8 items,
+// left the SMs busy 64% of the kernel's time at 20k: items differ in size and a CTA
+// lives as long as its largest.)
 __global__ void __launch_bounds__(256, PQ3D_VMIX_MINB)
-k_v_mixed(const VItem *__restrict__ vitems, int64_t n_vitems, const float *__restrict__ V32,
-          const __half *__restrict__ V16, const uint8_t *__restrict__ V8, const float *__restrict__ x, int xstride,
-          float *__restrict__ tpart)
+k_v_mixed(const VItemM *__restrict__ vitems, const int32_t *__restrict__ vwarp, int n_vwarp,
+          const VRowRec *__restrict__ recs, const float *__restrict__ V32, const __half *__restrict__ V16,
+          const uint8_t *__restrict__ V8, const float *__restrict__ x, int xstride, float *__restrict__ tpart)
 {
     asm volatile("griddepcontrol.launch_dependents;");
-    const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < n_vitems; w += nw) {
-        const VItem it = vitems[w];
+    const int w = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    if (w >= n_vwarp) return;
+    const int i1 = vwarp[w + 1];
+    for (int i = vwarp[w]; i < i1; ++i) {
+        const VItemM it = vitems[i];
         const int cls = it.s >> 8, slip = it.s & 255;
-        if (cls == 0) v_item<float, float>(it, slip, V32, x, xstride, tpart);
-        else if (cls == 1) v_item<__half, float>(it, slip, V16, x, xstride, tpart);
-        else v_item<uint8_t, float>(it, slip, V8, x, xstride, tpart);
+        if (cls == 0) v_item_m<float>(it, slip, V32, recs, x, xstride, tpart);
+        else if (cls == 1) v_item_m<__half>(it, slip, V16, recs, x, xstride, tpart);
+        else v_item_m<uint8_t>(it, slip, V8, recs, x, xstride, tpart);
     }
 }
 
@@ -1064,7 +1131,7 @@ struct HmPlan {
     const void *U;         // packed U factors
     const void *V;         // packed V factors
     const void *ditems;    // DenseItem[n_ditems]
-    const void *vitems;    // VItem[n_vitems]
+    const void *vitems;    // VItem[n_vitems] (storage code 3, plain kernels: VItemM)
     const void *utasks;    // UTask[n_utasks]
     const int32_t *leaf_of_row, *leaf_ptr, *leaf_off;
     int64_t n_ditems, n_vitems, n_utasks, n_slots, n_tpart;
@@ -1080,6 +1147,9 @@ struct HmPlan {
     float *tfull;                      // the blocks' t, written by k_t_gather
     int64_t n_gather;
     int32_t ncta_a, ncta_b;
+    const void *vrows;                 // storage code 3, plain kernels: VRowRec list of the VItemM items
+    const int32_t *vwarp;              // k_v_mixed's per-warp item lists (n_vwarp + 1 offsets)
+    int32_t n_vwarp, pad3;
 };
 
 PQ3D_EXPORT size_t pq3d_item_bytes(int kind)
@@ -1093,6 +1163,8 @@ PQ3D_EXPORT size_t pq3d_item_bytes(int kind)
     case 6: return sizeof(UTaskM);
     case 7: return sizeof(StreamTask);
     case 8: return sizeof(TGather);
+    case 9: return sizeof(VItemM);
+    case 10: return sizeof(VRowRec);
     }
     return 0;
 }
@@ -1157,10 +1229,10 @@ static int run_matvec_mixed(const HmPlan &P, const float *x, float *slots, float
                             const double *add1, const double *add2, double *y, cudaStream_t st)
 {
     if (P.n_vitems > 0) {
-        const int resident = vmix_ctas();
-        if (resident <= 0) return PQ3D_ERR_CUDA;
-        const int64_t blocks = std::min<int64_t>((P.n_vitems * 32 + 255) / 256, resident);
-        k_v_mixed<<<(unsigned)blocks, 256, 0, st>>>((const VItem *)P.vitems, P.n_vitems, (const float *)P.V,
+        if (!P.vrows || !P.vwarp || P.n_vwarp <= 0) return PQ3D_ERR_ARG;
+        const int blocks = (P.n_vwarp + 7) / 8;
+        k_v_mixed<<<(unsigned)blocks, 256, 0, st>>>((const VItemM *)P.vitems, P.vwarp, P.n_vwarp,
+                                                    (const VRowRec *)P.vrows, (const float *)P.V,
                                                     (const __half *)P.V16, (const uint8_t *)P.V8, x, x_stride(P.n),
                                                     tpart);
     }
@@ -1231,6 +1303,14 @@ static int run_matvec_stream(const HmPlan &P, const float *x, float *slots, floa
         k_rowsum<float><<<(P.n + 255) / 256, 256, 0, st>>>(P.n, P.leaf_of_row, P.leaf_ptr, P.leaf_off, slots, add0,
                                                            add1, add2, y);
     return pq3d_launch_status();
+}
+
+// Resident CTAs of k_v_mixed on this device: its plans' per-warp lists are made for
+// 8 warps per resident CTA.
+PQ3D_EXPORT int pq3d_vmix_ctas(void)
+{
+    const int v = vmix_ctas();
+    return v > 0 ? v : PQ3D_ERR_CUDA;
 }
 
 // Resident CTAs of the streamed kernel on this device (persistent grid size).

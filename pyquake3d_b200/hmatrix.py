@@ -367,7 +367,7 @@ def classify_terms(wS, wD, tol):
 
 
 def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chunk=32, u_rows=512, stream=False,
-                            ncta=148):
+                            ncta=148, nwarps=None):
     """Work items, slot layout and packing records of the mixed storage (code 3):
     FP32 dense items as in the FP32 plan; per low-rank block and term class c
     (FP32, FP16, INT8) the class's own U / V arrays with column groups MIXED_CW[c].
@@ -389,6 +389,7 @@ def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chu
     lr_bytes = 0
     kmax = 0
     counts = np.zeros((3, 2), np.int64)      # terms per (class, slip)
+    vgroups = {}                             # (column start, columns, class) -> the blocks' V rows
     for bi, b in enumerate(aca_blocks):
         m, nn = len(b.row.indices), len(b.col.indices)
         lo, hi = getattr(b, "rows", (0, m))
@@ -414,16 +415,14 @@ def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chu
             nch = _cdiv(ngv, gch)
             if stream and Qs[c] * 16 > _lib.STREAM_STAGE_BYTES:
                 raise _lib.Pq3dError("a block's term class has %d V rows, more than one stream stage holds" % Qs[c])
-            for ch in range(nch):
-                g0, g1 = ch * gch, min(ngv, (ch + 1) * gch)
-                if stream:
+            if stream:
+                for ch in range(nch):
+                    g0, g1 = ch * gch, min(ngv, (ch + 1) * gch)
                     vitems.append((v_off[c], Qs[c], 0, Qs[c], g0, g1, b.col.start - lead, (3 * ks[c]) | (c << 16),
                                    tp + ch * Qs[c]))
-                    continue
-                for s_, (qa, qb) in enumerate(((0, 3 * ks[c]), (3 * ks[c], Qs[c]))):
-                    for q in range(qa, qb, 32):
-                        vitems.append((v_off[c], Qs[c], q, min(32, qb - q), g0, g1, b.col.start - lead,
-                                       s_ | (c << 8), tp + ch * Qs[c]))
+            else:
+                # the block's V rows join those of the other blocks with the same columns
+                vgroups.setdefault((b.col.start, nn, c), []).append((v_off[c], Qs[c], 3 * ks[c], tp))
             rec_tp[c], rec_nch[c] = tp, nch
             tp += nch * Qs[c]
             if c:
@@ -440,14 +439,65 @@ def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chu
     A = _leaf_lists(struct, slot_rows)
     dense_entries = int(np.sum(dense_recs["m"].astype(np.int64) * dense_recs["n"])) if len(dense_recs) else 0
     n = struct.n
+    vrows = vwarp = None
     if not stream:
-        # k_v_mixed's warps stride through the items: largest first evens out their work
-        vitems.sort(key=lambda v: -v[3] * (v[5] - v[4]))
-    A.update(ditems=_rec(ditems, _lib.DENSE_ITEM), vitems=_rec(vitems, _lib.V_ITEM),
-             utasks=_rec(utasks, _lib.U_TASK_M), n_ditems=len(ditems), n_vitems=len(vitems), n_utasks=len(utasks),
+        if max(v_off) >= 1 << 32:
+            raise _lib.Pq3dError("a V class array of the mixed storage holds 2^32 elements or more")
+        vitems, vwarp, vrows = _merged_v_items(vgroups, v_chunk, nwarps or VMIX_WARPS)
+    A.update(ditems=_rec(ditems, _lib.DENSE_ITEM), vitems=_rec(vitems, _lib.V_ITEM_M if not stream else _lib.V_ITEM),
+             vrows=vrows, vwarp=vwarp, utasks=_rec(utasks, _lib.U_TASK_M), n_ditems=len(ditems), n_vitems=len(vitems), n_utasks=len(utasks),
              n_slots=slot, n_tpart=tp, n_scales=sb, kmax=kmax, u_sizes=u_off, v_sizes=v_off, pack=pack, stream=stream,
              class_terms=counts, alg_bytes=dense_entries * 6 * 4 + lr_bytes + 2 * n * 4 + 3 * n * 8)
     return A
+
+
+VMIX_WARPS = 8 * 148 * 6      # k_v_mixed warps when no device says otherwise (B200, 6 CTAs per SM)
+
+
+def _merged_v_items(vgroups, v_chunk, nwarps=VMIX_WARPS):
+    """V items of the mixed storage's plain kernels (k_v_mixed): for each column
+    cluster, class and slip, the V rows of all low-rank blocks with those columns
+    (in block order), per column chunk, 32 rows to an item, so the x slice is loaded
+    once for all of them.  vgroups: (column start, columns, class) -> [(V offset of
+    the block in its class array, Q, strike rows, t base)].  Returns the items
+    ordered by warp, the per-warp offsets (nwarps + 1) and the row records.  Items go
+    largest first to the least loaded of the nwarps warps (cost: row slots of 8 x
+    column groups, plus a fixed start), so the persistent warps end together."""
+    items, recs = [], []
+    for (col0, nn, c), blocks in vgroups.items():
+        cw = MIXED_CW[c]
+        lead = col0 % cw
+        ngv = _cdiv(nn + lead, cw)
+        nch = _cdiv(ngv, v_chunk)
+        for s_ in (0, 1):
+            rows = [(off, Q, q, tp) for off, Q, ks3, tp in blocks
+                    for q in (range(0, ks3) if s_ == 0 else range(ks3, Q))]
+            if not rows:
+                continue
+            for ch in range(nch):
+                g0, g1 = ch * v_chunk, min(ngv, (ch + 1) * v_chunk)
+                for r in range(0, len(rows), 32):
+                    part = rows[r:r + 32]
+                    items.append((len(recs), len(part), g0, g1, col0 - lead, s_ | (c << 8), 0))
+                    recs.extend((off + q * cw, Q * cw, tp + ch * Q + q) for off, Q, q, tp in part)
+    import heapq
+    cost = [((nr + 7) // 8) * (g1 - g0) + 16 for _, nr, g0, g1, _, _, _ in items]
+    order = sorted(range(len(items)), key=lambda i: -cost[i])
+    nwarps = max(8, min(int(nwarps), max(len(items), 1)) // 8 * 8)
+    heap = [(0, w) for w in range(nwarps)]
+    lists = [[] for _ in range(nwarps)]
+    for i in order:
+        load, w = heapq.heappop(heap)
+        lists[w].append(i)
+        heapq.heappush(heap, (load + cost[i], w))
+    vwarp = np.zeros(nwarps + 1, dtype=np.int32)
+    vwarp[1:] = np.cumsum([len(l) for l in lists])
+    items = [items[i] for l in lists for i in l]
+    rec = np.zeros(max(len(recs), 1), dtype=_lib.V_ROW)
+    if recs:
+        a = np.array(recs, dtype=np.int64)
+        rec["base"], rec["stride"], rec["out"] = a[:, 0], a[:, 1], a[:, 2]
+    return items, vwarp, rec
 
 
 def _balance(tasks, nbytes, ncta):
@@ -990,7 +1040,9 @@ class DeviceHMatrix:
                                                    ncta=ncta)
                 except _lib.Pq3dError:
                     pass               # a term class too large for a stream stage: the plain kernels
-        return build_plan_arrays_mixed(self.s, self.dense_recs, cls_lists, dc, vc, ur)
+        nw = self.L.pq3d_vmix_ctas()
+        return build_plan_arrays_mixed(self.s, self.dense_recs, cls_lists, dc, vc, ur,
+                                       nwarps=8 * nw if nw > 0 else VMIX_WARPS)
 
     def install_mixed(self, tmap, U, V, scales):
         """Register a mixed plan whose class arrays come from elsewhere (an operator
@@ -1047,6 +1099,11 @@ class DeviceHMatrix:
             hp["status"] = P["status"].data_ptr()
             hp["stream"] = 1 if A.get("stream") else 0
             P["stream"] = bool(A.get("stream"))
+            if not P["stream"]:
+                P["vrows"] = dev_rec(A["vrows"])
+                hp["vrows"] = P["vrows"].data_ptr()
+                P["vwarp"] = torch.tensor(A["vwarp"], dtype=torch.int32, device=self.dev)
+                hp["vwarp"], hp["n_vwarp"] = P["vwarp"].data_ptr(), len(A["vwarp"]) - 1
             if P["stream"]:
                 for k in ("tasks_a", "tasks_b", "gather"):
                     P[k] = dev_rec(A[k])

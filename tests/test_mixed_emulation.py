@@ -93,7 +93,8 @@ def pack_mixed(st, op, tol, stream=False):
     R = _near_rowabs(st, op)
     W = _weights(st, op, R)
     cls_lists = [classify_terms(wS, wD, tol) for wS, wD in W]
-    A = build_plan_arrays_mixed(st, recs, cls_lists, dense_chunk=2, v_chunk=3, u_rows=40, stream=stream, ncta=5)
+    A = build_plan_arrays_mixed(st, recs, cls_lists, dense_chunk=2, v_chunk=3, u_rows=40, stream=stream, ncta=5,
+                                nwarps=16)
     dt, fill = (np.float32, np.float16, np.uint8), (0, 0, 128)      # INT8 entries stored as b + 128
     U = [np.full(max(A["u_sizes"][c], 16), fill[c], dt[c]) for c in range(3)]
     V = [np.full(max(A["v_sizes"][c], 16), fill[c], dt[c]) for c in range(3)]
@@ -241,20 +242,25 @@ def emulate(st, A, D, U, V, scales, x):
                         acc[:, c] += D[it["off"] + ((g * 6 + 2 * c + s) * m + rr) * 4 + t] * \
                             x[2 * (int(it["c0"]) + g * 4 + t) + s]
         slots[3 * (int(it["slot"]) + rr)[:, None] + np.arange(3)] = acc
-    for it in A["vitems"][:A["n_vitems"]]:
-        cls, kS3 = int(it["s"]) >> 8, None
+    # merged V items: rows (one class, one slip) of the blocks sharing a column cluster,
+    # each row with its own class-array base, group stride and t index
+    written = np.zeros(len(tpart), dtype=bool)
+    vw = A["vwarp"]                       # k_v_mixed's per-warp item lists
+    assert vw[0] == 0 and vw[-1] == A["n_vitems"] and np.all(np.diff(vw) >= 0)
+    for it in (A["vitems"][i] for w in range(len(vw) - 1) for i in range(vw[w], vw[w + 1])):
+        cls, slip = int(it["s"]) >> 8, int(it["s"]) & 255
         cw = MIXED_CW[cls]
-        assert int(it["c0"]) % cw == 0
-        Q, q0, nr = int(it["Q"]), int(it["q"]), int(it["nr"])
-        for q in range(q0, q0 + nr):
-            slip = (0 if q < kS3 else 1) if kS3 is not None else int(it["s"]) & 255
+        assert int(it["c0"]) % cw == 0 and 0 < int(it["nr"]) <= 32
+        for R in A["vrows"][int(it["rows"]):int(it["rows"]) + int(it["nr"])]:
             acc = 0.0
             for g in range(int(it["g0"]), int(it["g1"])):
-                idx = it["off"] + (g * Q + q) * cw + np.arange(cw)
+                idx = int(R["base"]) + g * int(R["stride"]) + np.arange(cw)
                 assert idx.max() < len(V[cls])
                 acc += float(np.dot(_decode(V[cls][idx], cls),
                                     x[(2 + slip) * x_stride(st.n) + int(it["c0"]) + g * cw + np.arange(cw)]))
-            tpart[int(it["tp"]) + q] = acc
+            assert not written[int(R["out"])]          # every partial written once
+            written[int(R["out"])] = True
+            tpart[int(R["out"])] = acc
     for T in A["utasks"][:A["n_utasks"]]:
         m = int(T["m"])
         rr = np.arange(int(T["r0"]), int(T["r1"]))
