@@ -232,7 +232,9 @@ def accuracy_study(sim, op, nrep, precisions=("bf16",), marks=(50, 100, 200, 500
     """Relative L2 errors of slip, V, psi and theta of each precision against the FP64
     operator at equal times (dt replay of the FP64 run), after each mark; plus the FP64
     chaos floor: the same errors between two FP64 runs whose initial shear tractions
-    (both components) differ by a relative 1e-12.  The FP64 device path itself is pinned to the oracle's
+    (both components) differ by a relative 1e-12, and the same with a relative 2^-24
+    (FP32 unit roundoff: how far the fault's own dynamics carry a difference of the
+    size FP32 storage makes).  The FP64 device path itself is pinned to the oracle's
     simu_forward on the same operator (the cpu_baseline leg and the GPU tests)."""
     import torch
     from pyquake3d_b200.qdsim import DeviceStepper
@@ -251,32 +253,80 @@ def accuracy_study(sim, op, nrep, precisions=("bf16",), marks=(50, 100, 200, 500
     marks = [m for m in marks if m <= nrep] or [nrep]
     ref = DeviceStepper(sim, op, "fp64")
     others = {p: DeviceStepper(sim, op, p) for p in precisions if p in op.plans}
-    pert = DeviceStepper(sim, op, "fp64")
-    pert.t["Tt1o"].mul_(1.0 + 1e-12)           # both shear components: a pure-dip or pure-strike
-    pert.t["Tt2o"].mul_(1.0 + 1e-12)           # fault has one of them zero
-    for st in [ref, pert] + list(others.values()):
+    perts = {}
+    for name, eps in (("fp64_perturbed_1e-12", 1e-12), ("fp64_perturbed_2^-24", 2.0 ** -24)):
+        st = DeviceStepper(sim, op, "fp64")
+        st.t["Tt1o"].mul_(1.0 + eps)           # both shear components: a pure-dip or pure-strike
+        st.t["Tt2o"].mul_(1.0 + eps)           # fault has one of them zero
+        perts[name] = st
+    for st in [ref] + list(perts.values()) + list(others.values()):
         st.ctrl[0] = sim.htry
     ref.set_history(nrep)
-    out = {p: [] for p in others}
-    out["fp64_perturbed_1e-12"] = []
+    out = {p: [] for p in list(others) + list(perts)}
     done = 0
     for mk in marks:
         for i in range(done, mk):
             ref.launch(i)
         torch.cuda.synchronize()
         h = ref.hist.view(-1, 6)[:, 0]
-        for name, st in list(others.items()) + [("fp64_perturbed_1e-12", pert)]:
+        for name, st in list(others.items()) + list(perts.items()):
             st.set_replay(h)
             for i in range(done, mk):
                 st.launch(i)
         torch.cuda.synchronize()
-        for name, st in list(others.items()) + [("fp64_perturbed_1e-12", pert)]:
+        for name, st in list(others.items()) + list(perts.items()):
             e = errs(st, ref)
             e["steps"] = mk
             out[name].append(e)
         done = mk
     out["method"] = "dt replay of the FP64 run; relative L2 over elements"
     out["sim_time_s"] = float(ref.hist.view(-1, 6)[done - 1, 2])
+    return out
+
+
+def accuracy_common_times(sim, op, prec, nrep, marks=(100, 200, 500)):
+    """The second parity measure: FP64 and `prec` each step with their own controller;
+    at the FP64 run's times after each mark the `prec` run's slip, V and theta are
+    interpolated linearly in time between its two bracketing steps, and relative L2
+    errors over elements are formed against the FP64 state at that time."""
+    import torch
+    from pyquake3d_b200.qdsim import DeviceStepper
+
+    def fields(st):
+        return {"slip": torch.sqrt(st.t["slip1"] ** 2 + st.t["slip2"] ** 2), "V": st.t["slipv"].clone(),
+                "theta": st.t["dc"] / st.V0 * torch.exp((st.t["psi"] - st.t["f0"]) / st.t["b"])}
+
+    marks = [m for m in marks if m <= nrep] or [nrep]
+    ref = DeviceStepper(sim, op, "fp64")
+    ref.ctrl[0] = sim.htry
+    targets = []
+    done = 0
+    for mk in marks:
+        for i in range(done, mk):
+            ref.launch(i)
+        done = mk
+        targets.append((mk, float(ref.ctrl[2].item()), fields(ref)))
+    st = DeviceStepper(sim, op, prec)
+    st.ctrl[0] = sim.htry
+    prev_t, prev_f = 0.0, fields(st)
+    out = []
+    i = 0
+    for mk, t_ref, f_ref in targets:
+        while True:
+            t_now = float(st.ctrl[2].item())
+            if t_now >= t_ref:
+                break
+            prev_t, prev_f = t_now, fields(st)
+            st.launch(i)
+            i += 1
+            if i > 10 * nrep:
+                raise RuntimeError("the %s run fell behind the FP64 run's time" % prec)
+        cur = fields(st)
+        w = (t_ref - prev_t) / (t_now - prev_t) if t_now > prev_t else 1.0
+        e = {k: float(torch.linalg.norm(prev_f[k] + w * (cur[k] - prev_f[k]) - f_ref[k]) / torch.linalg.norm(f_ref[k]))
+             for k in f_ref}
+        e.update(steps_fp64=mk, steps=i, time_s=t_ref)
+        out.append(e)
     return out
 
 
@@ -352,6 +402,7 @@ def config_study(case, prec, nsteps, cpu_budget, marks, extra=()):
         acc = accuracy_study(sim, op, nsteps, precisions=tuple(low), marks=marks)
         out["err_vs_fp64"] = {p: acc[p] for p in low}
         out["fp64_chaos_floor"] = acc["fp64_perturbed_1e-12"]
+        out["fp64_perturbed_fp32_roundoff"] = acc["fp64_perturbed_2^-24"]
     ho = export_host_operator(op)
     crate, k, secs, ost, hs = cpu_reference_steps(ho, qd_oracle.sim_state(sim), sim.V0, sim.mu, sim.Cs, cpu_budget,
                                                   max_steps=200, dttry=sim.htry, reltol=sim.RelTol, fix_tn=sim.fix_Tn)
@@ -966,6 +1017,8 @@ def main():
     # accuracy vs the FP64 path at equal times (dt replay of the FP64 run), at several horizons
     # (a fixed horizon, independent of the timed step count)
     accuracy = accuracy_study(sim, op, args.accuracy_steps, precisions=("bf16", "fp32", "mixed"))
+    # the same comparison at common times, each run with its own step sizes
+    accuracy["common_times"] = {p: accuracy_common_times(sim, op, p, args.accuracy_steps) for p in ("fp32", "mixed")}
 
     # V-mode: DP5(4) with one H-matvec per stage and a Newton solve for V; MLP seed
     # trained on the run's own solves (hand-written kernels)
