@@ -1,6 +1,7 @@
 """Host logic against the reference run on the tiny case: mesh reading, element
 frames, initial conditions and the H-matrix block structure."""
 import numpy as np
+import pytest
 
 from pyquake3d_b200 import read_mshV2, get_eleVec
 from pyquake3d_b200.hmatrix import HStructure, aca_start_indices
@@ -80,3 +81,50 @@ def test_plan_cache_picks_entry_of_nearest_size(tmp_path, monkeypatch):
     assert hmatrix.plan_cache_entry("GPU X", "mixed", 2000)["v_chunk"] == 64
     assert hmatrix.plan_cache_entry("GPU X", "bf16", 2000) is None
     assert hmatrix.plan_cache_entry("GPU Y", "fp32", 2000) is None
+
+
+def test_prefetch_copier_hands_out_fresh_copies():
+    """The reference loop's attribute reads go through the host copier: every read of
+    every step gets its own array (the loop keeps them all), equal to the pinned
+    buffer at that step even after the buffer is overwritten, and an error in the
+    wait reaches the reader."""
+    import threading
+    from pyquake3d_b200 import qdsim
+
+    class NoDevice(qdsim._PrefetchCopier):
+        def _bind(self, device_index):
+            pass
+
+    class Done:
+        def __init__(self):
+            self.ev = threading.Event()
+
+        def synchronize(self):
+            self.ev.wait(5.0)
+
+    n = 1000
+    c = NoDevice(n, 0, spare=4)
+    buf = {"slipv": np.zeros(n), "Tt": np.zeros(n)}
+    kept = []
+    for step in range(20):
+        buf["slipv"][:] = step
+        buf["Tt"][:] = -step
+        d = Done()
+        job = c.submit(d, buf, ("Tt", "slipv"))
+        d.ev.set()
+        assert job.has("slipv") and job.has("Tt")
+        v, t = job.get("slipv"), job.get("Tt")
+        assert not job.has("slipv")
+        kept.append((step, v, t))
+    for step, v, t in kept:
+        assert np.all(v == step) and np.all(t == -step)
+    assert len({id(v) for _, v, _ in kept}) == len(kept)
+
+    class Bad:
+        def synchronize(self):
+            raise RuntimeError("wait failed")
+
+    job = c.submit(Bad(), buf, ("slipv",))
+    with pytest.raises(RuntimeError):
+        job.get("slipv")
+    c.stop()
