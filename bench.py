@@ -1062,7 +1062,7 @@ def main():
     # the reference main loop verbatim (src/main.py:161-184): after every step it reads
     # max |slipv1|, max |slipv2| and keeps the slipv and Tt arrays (device-backed QDsim
     # attributes, prefetched by the step after the first reads)
-    nl = min(args.steps, 100)
+    nl = min(args.steps, 300)
     _, dttry = sim.simu_forward(dttry)
     _ = (sim.slipv1, sim.slipv2, sim.slipv, sim.Tt)
     torch.cuda.synchronize()

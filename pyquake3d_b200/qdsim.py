@@ -535,17 +535,21 @@ class _PrefetchCopier:
     for each step's copy to land and copies every vector into one of them, while the
     device already runs the next step's H-matvec.  A read then waits only for its own
     vector.  (With one thread doing both, the page touching sat in the copies' path:
-    1,680-1,850 steps/s at 60k against 1,970-1,985 with two, and 1,280-1,370 with the
-    copies made by the reading thread.)"""
+    1,680-1,850 steps/s at 60k against 1,970-1,985 with a separate maker thread, and
+    1,280-1,370 with the copies made by the reading thread.)"""
 
-    def __init__(self, n, device_index, spare=12):
+    def __init__(self, n, device_index, spare=16, makers=2):
         self.n = n
         self.q = queue.Queue()
         self.pool = queue.Queue(maxsize=spare)
         self.stopped = False
         self.thread = threading.Thread(target=self._run, args=(device_index,), daemon=True)
-        self.maker = threading.Thread(target=self._make, daemon=True)
-        self.maker.start()
+        # the loop takes four fresh 8n-byte arrays per step; one maker thread kept up at
+        # 60k on B200 hosts (1,956-1,968 steps/s with one or two), the second is headroom
+        # for hosts whose page faults are slower
+        self.makers = [threading.Thread(target=self._make, daemon=True) for _ in range(makers)]
+        for t in self.makers:
+            t.start()
         self.thread.start()
 
     def submit(self, done, views, names):
