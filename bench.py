@@ -740,7 +740,7 @@ def run_partition(args, rank, world, local):
     # warm-up (device-controlled, one host read at the end), then the graph
     ps.run_device(args.warmup, sim.htry, chunk=args.warmup)
     G = 50
-    graph = ps.capture(G) if args.steps % G == 0 else None
+    graph = ps.capture(G)
     ok = max_over_ranks(0.0 if graph is not None else 1.0) == 0.0
     if not ok:
         graph = None                       # every rank launches alike
@@ -752,28 +752,36 @@ def run_partition(args, rank, world, local):
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # G steps per replay (or G eager steps), then one host read of the control block; a
+    # step that needed more than the attempt slots halted the device sequence and is
+    # finished here by the host controller, inside the timed region, before the next
+    # chunk: every rank reads the same block and takes the same path
     e0.record()
-    if graph is not None:
-        for _ in range(args.steps // G):
+    done, halts = 0, 0
+    prev = int(pc0[P.PC_STEPS])
+    while done < args.steps:
+        if graph is not None:
             graph.replay()
-    else:
-        for _ in range(args.steps):
-            ps.enqueue_device_step()
+        else:
+            for _ in range(G):
+                ps.enqueue_device_step()
+        pc1 = be.pc.cpu().numpy()
+        if pc1[P.PC_STATUS] != 0:
+            raise RuntimeError("time step failed in the partitioned run")
+        done += int(pc1[P.PC_STEPS]) - prev
+        if pc1[P.PC_HALT] != 0:
+            halts += 1
+            ps.time, ps.steps, ps.rejects = float(pc1[P.PC_TIME]), int(pc1[P.PC_STEPS]), int(pc1[P.PC_REJ])
+            h, dtnext = ps._attempts(float(pc1[P.PC_H]), int(pc1[P.PC_NRJCT]), False)
+            be.pc_resume(ps, dtnext, h)
+            done += 1
+        prev = int(be.pc[P.PC_STEPS].item())
     e1.record()
     torch.cuda.synchronize()
     barrier()
     clocks = clk.stop()
     t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
-    pc1 = be.pc.cpu().numpy()
-    done = int(pc1[P.PC_STEPS] - pc0[P.PC_STEPS])
-    halted = bool(pc1[P.PC_HALT] != 0)
-    if pc1[P.PC_STATUS] != 0:
-        raise RuntimeError("time step failed in the partitioned run")
-    if halted:
-        # the halted step and the rest of the timed count, outside the timed region
-        ps.time, ps.steps, ps.rejects = float(pc1[P.PC_TIME]), int(pc1[P.PC_STEPS]), int(pc1[P.PC_REJ])
-        h, dtnext = ps._attempts(float(pc1[P.PC_H]), int(pc1[P.PC_NRJCT]), False)
-        be.pc_resume(ps, dtnext, h)
+    halted = halts > 0
     del graph                              # holds NCCL calls: released before the group
 
     # this rank's H-matvec alone (its rows' blocks), CUDA events
@@ -818,10 +826,10 @@ def run_partition(args, rank, world, local):
                    "parallelism": "row partition x%d" % world, "precision": args.precision,
                    "collectives": "NCCL" if dist.is_initialized() else "none (one rank, one process)",
                    "rows_per_rank": [int(b[r + 1] - b[r]) for r in range(world)],
-                   "attempt_slots": args.attempts, "cuda_graph_steps": G if ok and args.steps % G == 0 else 0,
+                   "attempt_slots": args.attempts, "cuda_graph_steps": G if ok else 0,
                    "l2": "inputs larger than L2 (operator %.2f GB per step over all ranks)" % (bytes_all / 1e9),
                    "host_setup_s": round(t_host, 2), "assembly_s": round(t_asm, 2)},
-        "steps_done": done, "halted": halted,
+        "steps_done": done, "halted": halted, "host_finished_steps": halts,
         "roofline": {"bound": "hbm", "achieved": bytes_all / t_mv / 1e9, "peak": hbm * world, "unit": "GB/s",
                      "frac": bytes_all / t_mv / 1e9 / (hbm * world), "traffic": None,
                      "kernel": "H-matvec of every rank's rows (slowest rank's time), %d GPUs" % world,

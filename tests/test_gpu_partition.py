@@ -129,3 +129,26 @@ def test_device_controller_halts_and_host_finishes(lib, tiny_files, tiny_golden,
     for x, y in zip(ba, bb):
         np.testing.assert_allclose(x.get("slip1"), y.get("slip1"), rtol=1e-12, atol=1e-300)
         np.testing.assert_allclose(x.get("psi"), y.get("psi"), rtol=1e-12)
+
+
+def test_bench_partition_arm(lib):
+    """bench.py's row-partition arm (what `bench.py --gpus N` runs) on one GPU and one
+    rank, thrust20k: the timed region completes its steps (graph replays of 50 steps,
+    any step that outran the attempt slots finished by the host controller inside the
+    region) and the JSON line carries the strong-scaling fields."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "TORCHELASTIC_RUN_ID")}
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--parallelism", "partition", "--case",
+                        "thrust20k", "--steps", "50", "--warmup", "3", "--no-cpu"], cwd=root, env=env,
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["scaling"] == "strong" and line["n_gpus"] == 1
+    assert line["steps_done"] >= 50 and line["value"] > 0
+    assert line["halted"] == (line["host_finished_steps"] > 0)
+    assert line["config"]["cuda_graph_steps"] == 50
+    assert line["gpu_launches"] > 0 and line["e2e"]["value"] > 0
