@@ -452,6 +452,7 @@ def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chu
 
 
 VMIX_WARPS = 8 * 148 * 6      # k_v_mixed warps when no device says otherwise (B200, 6 CTAs per SM)
+VMIX_ROWS = 32                # rows per merged V item (k_v_mixed handles up to 32)
 
 
 def _merged_v_items(vgroups, v_chunk, nwarps=VMIX_WARPS):
@@ -476,8 +477,8 @@ def _merged_v_items(vgroups, v_chunk, nwarps=VMIX_WARPS):
                 continue
             for ch in range(nch):
                 g0, g1 = ch * v_chunk, min(ngv, (ch + 1) * v_chunk)
-                for r in range(0, len(rows), 32):
-                    part = rows[r:r + 32]
+                for r in range(0, len(rows), VMIX_ROWS):
+                    part = rows[r:r + VMIX_ROWS]
                     items.append((len(recs), len(part), g0, g1, col0 - lead, s_ | (c << 8), 0))
                     recs.extend((off + q * cw, Q * cw, tp + ch * Q + q) for off, Q, q, tp in part)
     import heapq
