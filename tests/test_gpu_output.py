@@ -1,7 +1,8 @@
 """GPU: operator checkpoint round trip and the command-line driver on the tiny case.
 
 * a checkpointed operator, loaded into a fresh DeviceHMatrix, gives bitwise the
-  same products as the assembled one, for every stored precision;
+  same products as the assembled one, for every stored precision (the mixed
+  storage's term classes, class arrays and scales included);
 * the driver (pyquake3d_b200.main.run) follows the reference's 30-step dt sequence
   (state.txt, %f of h), writes Init.vtk, out_vtk/stepI.vtk and the per-step slip
   rate / traction dumps of the reference layout, and a second run that loads the
@@ -31,14 +32,14 @@ def test_checkpoint_roundtrip_bitwise(lib, tiny_sim, tiny_golden, tmp_path):
     s = tiny_sim
     kw = dict(aca_tol=0.01, aca_rel=False, aca_seed=int(tiny_golden["aca_seed"]))
     op = DeviceHMatrix(s.tree_block.struct, s.xg, s.eleVec, s.nodelst, s.elelst, s.mu, s.lambda_, **kw)
-    op.assemble(("fp64", "fp32", "bf16"))
+    op.assemble(("fp64", "fp32", "bf16", "mixed"))
     p = str(tmp_path / checkpoint.FILE_NAME)
     checkpoint.save_operator(op, p, s.xg, s.eleVec)
     op2 = DeviceHMatrix(s.tree_block.struct, s.xg, s.eleVec, s.nodelst, s.elelst, s.mu, s.lambda_, **kw)
     checkpoint.load_operator(op2, p, s.xg, s.eleVec)
     rng = np.random.default_rng(3)
     x1, x2 = rng.standard_normal((2, s.xg.shape[0])) * 1e-9
-    for d in ("fp64", "fp32", "bf16"):
+    for d in ("fp64", "fp32", "bf16", "mixed"):
         a = op.apply(x1, x2, d)
         b = op2.apply(x1, x2, d)
         for u, v in zip(a, b):
