@@ -395,11 +395,12 @@ k_u(const UTask *__restrict__ tasks, const TL *__restrict__ U, const TA *__restr
 
 // ------------------------------------------------------------------ mixed storage
 // Resident CTAs per SM the register allocation of k_v_mixed / k_du_mixed is held to
-// (measured on B200 at 60k, mixed matvec: 6 and 5 give 0.483 ms against 0.672 ms for
+// (measured on B200 at 60k, mixed matvec: 6 and 5 gave 0.483 ms against 0.672 ms for
 // the compiler's own choice at one CTA per SM and 0.499 ms for 5 and 5; both kernels are
-// latency-bound streams, so occupancy matters more than a few spilled registers).
+// latency-bound streams.  With the INT8 V loop below, k_v_mixed at 4 CTAs (64 registers,
+// no spill in its loops) beats 5 and 6: 440.9 / 444.6 / 460.1 us per 60k matvec).
 #ifndef PQ3D_VMIX_MINB
-#define PQ3D_VMIX_MINB 6
+#define PQ3D_VMIX_MINB 4
 #endif
 #ifndef PQ3D_UMIX_MINB
 #define PQ3D_UMIX_MINB 5
@@ -532,25 +533,43 @@ __device__ __forceinline__ void v_item_m(const VItemM &it, int slip, const TL *_
         const float *xp = x + (int64_t)(2 + slip) * xstride + it.c0 + (int64_t)(it.g0 + jg) * CWV;  // CWV-aligned
 #pragma unroll 2
         for (int g = it.g0 + jg; g < it.g1; g += 4) {
-            float xs[CWV];
-            ld_vec<float, CWV>(xp, xs);
+            if constexpr (std::is_same<TL, uint8_t>::value) {
+                // INT8: the rows' units first, then x four values at a time (4 live registers
+                // instead of 16 for the slice); per row the summation order of the other
+                // classes' loop (column t, then its four entries).  Units of rows beyond nu
+                // hold the byte 128, which decodes to zero, and are never stored.
+                // (Measured at 60k: V products 205 -> 153 us, mixed matvec 460 -> 441 us.)
+                Vec16<TL> d[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (u < nu) {
-                    Vec16<TL> d = ld_stream(Vd + off[u]);
-                    if constexpr (std::is_same<TL, uint8_t>::value) {
+                for (int u = 0; u < 4; ++u) {
+                    if (u < nu) d[u] = ld_stream(Vd + off[u]);
+                    else d[u].w[0] = d[u].w[1] = d[u].w[2] = d[u].w[3] = 0x80808080u;
+                }
+                const float4 *x4 = reinterpret_cast<const float4 *>(xp);
 #pragma unroll
-                        for (int t = 0; t < 4; ++t) {
-                            acc[u] += i8_at<0>(d.w[t]) * xs[4 * t];
-                            acc[u] += i8_at<1>(d.w[t]) * xs[4 * t + 1];
-                            acc[u] += i8_at<2>(d.w[t]) * xs[4 * t + 2];
-                            acc[u] += i8_at<3>(d.w[t]) * xs[4 * t + 3];
-                        }
-                    } else {
+                for (int t = 0; t < 4; ++t) {
+                    const float4 xv = __ldg(x4 + t);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        acc[u] += i8_at<0>(d[u].w[t]) * xv.x;
+                        acc[u] += i8_at<1>(d[u].w[t]) * xv.y;
+                        acc[u] += i8_at<2>(d[u].w[t]) * xv.z;
+                        acc[u] += i8_at<3>(d[u].w[t]) * xv.w;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) off[u] += st4[u];
+            } else {
+                float xs[CWV];
+                ld_vec<float, CWV>(xp, xs);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (u < nu) {
+                        Vec16<TL> d = ld_stream(Vd + off[u]);
 #pragma unroll
                         for (int t = 0; t < CWV; ++t) acc[u] += widen<float>(d.v[t]) * xs[t];
+                        off[u] += st4[u];
                     }
-                    off[u] += st4[u];
                 }
             }
             xp += 4 * CWV;

@@ -451,7 +451,7 @@ def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chu
     return A
 
 
-VMIX_WARPS = 8 * 148 * 6      # k_v_mixed warps when no device says otherwise (B200, 6 CTAs per SM)
+VMIX_WARPS = 8 * 148 * 4      # k_v_mixed warps when no device says otherwise (B200, 4 CTAs per SM)
 VMIX_ROWS = 32                # rows per merged V item (k_v_mixed handles up to 32)
 
 
