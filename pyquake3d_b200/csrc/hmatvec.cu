@@ -402,11 +402,14 @@ k_u(const UTask *__restrict__ tasks, const TL *__restrict__ U, const TA *__restr
 #ifndef PQ3D_VMIX_MINB
 #define PQ3D_VMIX_MINB 4
 #endif
+// k_du_mixed at 4 (in 256-thread units: 8 CTAs of 128 threads, 64 registers) with three U
+// column groups in flight: 60k 438.0 -> 434.9 us, 20k 94.5 -> 93.8 us against 5 and two
+// (its dense items gain, 183 -> 172 us alone, its U tasks lose, 131 -> 138 us).
 #ifndef PQ3D_UMIX_MINB
-#define PQ3D_UMIX_MINB 5
+#define PQ3D_UMIX_MINB 4
 #endif
 #ifndef PQ3D_UMIX_UNROLL
-#define PQ3D_UMIX_UNROLL 2
+#define PQ3D_UMIX_UNROLL 3
 #endif
 constexpr int kUmixUnroll = PQ3D_UMIX_UNROLL;     // column groups of a U row in flight
 // Storage code 3: FP32 dense near field; each low-rank block's ACA terms split
