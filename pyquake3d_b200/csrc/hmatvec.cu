@@ -644,9 +644,28 @@ k_du_mixed(const DenseItem *__restrict__ ditems, int64_t n_ditems, int64_t n_dbl
         dense_v_item<float, float, float>(w, ditems, n_ditems, nullptr, 0, D, nullptr, x, 0, slots, nullptr);
         return;
     }
+    // The task's U rows do not depend on the V kernel: start bringing them into L2 (one bulk
+    // prefetch per class, column group and component: rows [r0, r1), 16 B each) before
+    // waiting for the V partials and gathering t.  Measured at 60k: 432.7 -> 420.6 us per
+    // mixed matvec, 20k 93.9 -> 90.4 us (the prefetches run during the V kernel's tail).
+    const UTaskM T = tasks[blockIdx.x - n_dblocks];
+    const int nr = T.r1 - T.r0;
+    if (nr > 0) {
+        const int n0 = 3 * (T.K[0] / 4), n1 = 3 * (T.K[1] / 8), n2 = 3 * (T.K[2] / 16);
+        for (int e = threadIdx.x; e < n0 + n1 + n2; e += blockDim.x) {
+            const unsigned char *base;
+            int64_t off;
+            int q;
+            if (e < n0) { base = (const unsigned char *)U32; off = T.off[0] * 4; q = e; }
+            else if (e < n0 + n1) { base = (const unsigned char *)U16; off = T.off[1] * 2; q = e - n0; }
+            else { base = (const unsigned char *)U8; off = T.off[2]; q = e - n0 - n1; }
+            // run q = 3 g + c (column group g, component c) starts at unit (3 g + c) m + r0
+            const unsigned char *p = base + off + ((int64_t)q * T.m + T.r0) * 16;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(nr * 16) : "memory");
+        }
+    }
     asm volatile("griddepcontrol.wait;" ::: "memory");
     extern __shared__ __align__(16) unsigned char smraw[];
-    const UTaskM T = tasks[blockIdx.x - n_dblocks];
     u_task_mixed(T, U32, U16, U8, tpart, scales, slots, reinterpret_cast<float *>(smraw));
 }
 
