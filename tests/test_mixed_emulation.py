@@ -326,6 +326,37 @@ def test_mixed_matvec_emulation_within_bound(setup, tol, stream):
         assert sum(int((c == 2).sum()) for cs in cls for c in cs) > 0      # INT8 terms exercised
 
 
+@pytest.mark.parametrize("tol", [2.0 ** -22, 2.0 ** -16])
+def test_u_task_prefetch_runs_cover_the_task_reads(setup, tol):
+    """k_du_mixed's U-task CTAs prefetch their rows into L2 before waiting for the V kernel:
+    one bulk prefetch per (class, column group, component), starting at byte
+    off_c * size_c + ((3 g + c) m + r0) * 16 with length (r1 - r0) * 16.  Restated here:
+    every run lies inside its class array, starts 16-byte aligned, has a nonzero size that
+    is a multiple of 16, and the runs cover exactly the 16-byte units the task's rows read."""
+    st, op = setup
+    A, D, U, V, scales, R, cls = pack_mixed(st, op, tol)
+    size = (4, 2, 1)
+    for T in A["utasks"][:A["n_utasks"]]:
+        m, r0, r1 = int(T["m"]), int(T["r0"]), int(T["r1"])
+        nr = r1 - r0
+        assert nr > 0
+        for c in range(3):
+            cw, K, off = MIXED_CW[c], int(T["K"][c]), int(T["off"][c])
+            assert K % cw == 0
+            runs = set()
+            for q in range(3 * (K // cw)):                  # the kernel's run index e - n_prev
+                start = off * size[c] + (q * m + r0) * 16
+                assert start % 16 == 0 and nr * 16 > 0
+                assert start + nr * 16 <= len(U[c]) * size[c]
+                runs.update(range(start // 16, start // 16 + nr))
+            reads = set()
+            for g in range(K // cw):
+                for comp in range(3):
+                    e = off + ((g * 3 + comp) * m + np.arange(r0, r1)) * cw    # u_row_class's units
+                    reads.update((e * size[c] // 16).tolist())
+            assert runs == reads
+
+
 def test_classify_terms_keeps_required_precision():
     rng = np.random.default_rng(3)
     tol = 2.0 ** -22
