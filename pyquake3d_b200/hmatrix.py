@@ -394,8 +394,8 @@ def build_plan_arrays_mixed(struct, dense_recs, cls_lists, dense_chunk=16, v_chu
         m, nn = len(b.row.indices), len(b.col.indices)
         lo, hi = getattr(b, "rows", (0, m))
         cS, cD = cls_lists[bi]
-        ks = [int((cS == c).sum()) for c in range(3)]
-        kd = [int((cD == c).sum()) for c in range(3)]
+        ks = np.bincount(cS, minlength=3).tolist()
+        kd = np.bincount(cD, minlength=3).tolist()
         if sum(ks) + sum(kd) == 0:
             continue
         Ks = [_cdiv(ks[c] + kd[c], MIXED_CW[c]) * MIXED_CW[c] for c in range(3)]
@@ -465,22 +465,30 @@ def _merged_v_items(vgroups, v_chunk, nwarps=VMIX_WARPS):
     largest first to the least loaded of the nwarps warps (cost: row slots of 8 x
     column groups, plus a fixed start), so the persistent warps end together."""
     items, recs = [], []
+    nrec = 0
     for (col0, nn, c), blocks in vgroups.items():
         cw = MIXED_CW[c]
         lead = col0 % cw
         ngv = _cdiv(nn + lead, cw)
         nch = _cdiv(ngv, v_chunk)
+        bl = np.array(blocks, dtype=np.int64).reshape(-1, 4)     # off, Q, strike rows, t base
         for s_ in (0, 1):
-            rows = [(off, Q, q, tp) for off, Q, ks3, tp in blocks
-                    for q in (range(0, ks3) if s_ == 0 else range(ks3, Q))]
-            if not rows:
+            # the slip's rows of every block, in block order: q in [0, ks3) or [ks3, Q)
+            lo = np.zeros(len(bl), np.int64) if s_ == 0 else bl[:, 2]
+            cnt = (bl[:, 2] if s_ == 0 else bl[:, 1]) - lo
+            nrows = int(cnt.sum())
+            if nrows == 0:
                 continue
+            blk = np.repeat(np.arange(len(bl)), cnt)
+            q = np.arange(nrows) - np.repeat(np.cumsum(cnt) - cnt, cnt) + lo[blk]
+            off, Q, tp = bl[blk, 0], bl[blk, 1], bl[blk, 3]
             for ch in range(nch):
                 g0, g1 = ch * v_chunk, min(ngv, (ch + 1) * v_chunk)
-                for r in range(0, len(rows), VMIX_ROWS):
-                    part = rows[r:r + VMIX_ROWS]
-                    items.append((len(recs), len(part), g0, g1, col0 - lead, s_ | (c << 8), 0))
-                    recs.extend((off + q * cw, Q * cw, tp + ch * Q + q) for off, Q, q, tp in part)
+                for r in range(0, nrows, VMIX_ROWS):
+                    items.append((nrec + r, min(VMIX_ROWS, nrows - r), g0, g1, col0 - lead, s_ | (c << 8), 0))
+                # row records of this chunk's items, consecutive in item order
+                recs.append(np.stack([off + q * cw, Q * cw, tp + ch * Q + q], axis=1))
+                nrec += nrows
     import heapq
     cost = [((nr + 7) // 8) * (g1 - g0) + 16 for _, nr, g0, g1, _, _, _ in items]
     order = sorted(range(len(items)), key=lambda i: -cost[i])
@@ -494,9 +502,9 @@ def _merged_v_items(vgroups, v_chunk, nwarps=VMIX_WARPS):
     vwarp = np.zeros(nwarps + 1, dtype=np.int32)
     vwarp[1:] = np.cumsum([len(l) for l in lists])
     items = [items[i] for l in lists for i in l]
-    rec = np.zeros(max(len(recs), 1), dtype=_lib.V_ROW)
+    rec = np.zeros(max(nrec, 1), dtype=_lib.V_ROW)
     if recs:
-        a = np.array(recs, dtype=np.int64)
+        a = np.concatenate(recs)
         rec["base"], rec["stride"], rec["out"] = a[:, 0], a[:, 1], a[:, 2]
     return items, vwarp, rec
 
@@ -559,8 +567,8 @@ def _build_stream_mixed(struct, dense_recs, cls_lists, ncta):
         m, nn = len(b.row.indices), len(b.col.indices)
         lo, hi = getattr(b, "rows", (0, m))
         cS, cD = cls_lists[bi]
-        ks = [int((cS == c).sum()) for c in range(3)]
-        kd = [int((cD == c).sum()) for c in range(3)]
+        ks = np.bincount(cS, minlength=3).tolist()
+        kd = np.bincount(cD, minlength=3).tolist()
         if sum(ks) + sum(kd) == 0:
             continue
         Ks = [_cdiv(ks[c] + kd[c], MIXED_CW[c]) * MIXED_CW[c] for c in range(3)]
