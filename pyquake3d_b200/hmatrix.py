@@ -28,7 +28,7 @@ from ._lib import ptr, check
 
 
 class ClusterNode:
-    __slots__ = ("indices", "left", "right", "start", "level", "bbox_min", "bbox_max", "leaf_id")
+    __slots__ = ("indices", "left", "right", "start", "level", "bbox_min", "bbox_max", "leaf_id", "_box")
 
     def __init__(self, indices, level):
         self.indices = indices
@@ -38,6 +38,7 @@ class ClusterNode:
         self.level = level
         self.bbox_min = None
         self.bbox_max = None
+        self._box = None
         self.leaf_id = -1
 
 
@@ -101,11 +102,27 @@ def _fix_starts(root):
             nd.start = nd.left.start
 
 
+def _box(nd):
+    """(bbox_min, bbox_max as floats, diameter) of a cluster, computed once."""
+    if nd._box is None:
+        lo, hi = [float(v) for v in nd.bbox_min], [float(v) for v in nd.bbox_max]
+        e = [h - l for l, h in zip(lo, hi)]
+        nd._box = (lo, hi, math.sqrt((e[0] * e[0] + e[1] * e[1]) + e[2] * e[2]))
+    return nd._box
+
+
 def is_admissible(a, b, eta):
-    """min(diam_a, diam_b) <= eta * dist(bbox_a, bbox_b)."""
-    da = np.sqrt(np.sum((a.bbox_max - a.bbox_min) ** 2))
-    db = np.sqrt(np.sum((b.bbox_max - b.bbox_min) ** 2))
-    dq = np.sqrt(np.sum((np.maximum(0, b.bbox_min - a.bbox_max) ** 2) + (np.maximum(0, a.bbox_min - b.bbox_max) ** 2)))
+    """min(diam_a, diam_b) <= eta * dist(bbox_a, bbox_b).  The sums run in numpy's
+    order for three terms ((t0 + t1) + t2) and every operation is correctly rounded,
+    so the decisions are those of the reference's numpy expression."""
+    alo, ahi, da = _box(a)
+    blo, bhi, db = _box(b)
+    t = []
+    for k in range(3):
+        u = max(0.0, blo[k] - ahi[k])
+        v = max(0.0, alo[k] - bhi[k])
+        t.append(u * u + v * v)
+    dq = math.sqrt((t[0] + t[1]) + t[2])
     return min(da, db) <= eta * dq
 
 
